@@ -1,0 +1,336 @@
+#!/usr/bin/env python3
+"""Headline benchmark: PBF particle-substeps/s on one B200 (or N replicas).
+
+Workload (default): the large dam break, 4,194,304 particles (256x128x128
+lattice, d=0.005, h=0.01), box 2x1x1, 1 substep per dt=1/120, 4 solver
+iterations, static capsule SDF obstacle (r=0.1, axis z, x=1.2), FP32.  A
+"step" is one PBFluids::step() (= one substep here) over the whole scene.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Timing: W untimed steps, then exactly K steps between CUDA events recorded on
+the engine's stream, with a barrier + device synchronize on both sides; the
+maximum over ranks is reported.  The working set (~1.7 GB) is far larger than
+the 126 MB L2, so no flush is needed between steps.  For N > 1 every rank steps
+its own replica of the scene (the plain step does not shard; no collective).
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "realtime-fsi-engine_b200"))
+
+METRIC = "particle-substeps/s"
+# algorithmic bytes per particle and launch (payload only: vec3 = 12 B,
+# scalar = 4 B; each pass reads its inputs and writes its outputs once)
+ALGO_BYTES = {"predict_hash": 28, "radix_sort": 16, "cell_table": 12, "reorder": 64, "lambda": 16,
+              "deltap_apply": 28, "integrate": 72, "vorticity": 48}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=["c2", "c0"], default="c2")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---- distributed plumbing ------------------------------------------------------------
+class Dist:
+    def __init__(self, want):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", self.local))
+            self.pg = dist
+        if want != self.world and self.rank == 0:
+            print(f"warning: --gpus {want} but WORLD_SIZE={self.world}", file=sys.stderr)
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x):
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64, device=f"cuda:{self.local}")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.barrier()
+            self.pg.destroy_process_group()
+
+
+# ---- clocks ------------------------------------------------------------------------------
+class Clocks:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.proc = None
+        self.path = None
+        try:
+            import torch
+            uuid = "GPU-" + str(torch.cuda.get_device_properties(device).uuid)
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", uuid, f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        smax = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[4 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---- scenes ------------------------------------------------------------------------------
+def workload(name, sample=None):
+    from pbf_b200 import scenes
+    if name == "c0":
+        cfg, pos, vel = scenes.c0(32)
+        return cfg, pos, vel, None, "dam break 32^3 (32,768 particles, d=0.02, h=0.04, S=2, I=4)"
+    if sample:
+        cfg, pos, vel, sdf = scenes.c2(nx=sample[0], ny=sample[1], nz=sample[2])
+    else:
+        cfg, pos, vel, sdf = scenes.c2()
+    return cfg, pos, vel, sdf, ("dam break 256x128x128 (4,194,304 particles, d=0.005, h=0.01, S=1 at dt=1/120, I=4, "
+                                "capsule SDF r=0.1 at x=1.2)")
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+def traffic_summary():
+    """Per-launch DRAM bytes of the dominant kernel from a committed ncu
+    capture summary (profiles/traffic.json), scaled to the workload."""
+    try:
+        return json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+    except Exception:
+        return {}
+
+
+# ---- CPU reference / baseline -------------------------------------------------------------------
+def cpu_reference_rate(budget_s):
+    """The reference's own compute shaders, compiled as C++ and run with
+    OpenMP on the host cores (oracle/_ref), on a 64^3 sub-block of the same
+    workload; falls back to the FP64 oracle port when _ref is absent."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cfg, pos, vel, sdf, _ = workload("c2", sample=(64, 64, 64))
+    n = len(pos)
+    grid, origin, cell, pad = sdf
+    osdf = O.Sdf(grid, origin, cell, padding=pad, containment=False)
+    ocfg = O.FluidConfig()
+    C.memmove(C.byref(ocfg), C.byref(cfg), C.sizeof(ocfg))
+    cores = os.cpu_count() or 1
+    sample = f"64x64x64 sub-block of the 4M lattice ({n} particles, same d/h/constants/capsule)"
+    steps = 0
+    t0 = time.perf_counter()
+    if O.have_ref():
+        import pbf_b200 as P
+        d = O.DerivedParams()
+        C.memmove(C.byref(d), C.byref(P.derive_params(cfg)), C.sizeof(d))
+        S = O.GlslScene(d, ocfg, pos, vel, sdf=osdf, sort_mode=0, parallel=True, pre_integrate=True)
+        kind = "reference"
+        while True:
+            S.step()
+            steps += 1
+            if time.perf_counter() - t0 > budget_s or steps >= 50:
+                break
+    else:
+        kind = "port"
+        p = O.Params(ocfg)
+        p64, v64 = pos.astype(np.float64), vel.astype(np.float64)
+        while True:
+            O.step(p, p64, v64, sdf=osdf)
+            steps += 1
+            if time.perf_counter() - t0 > budget_s or steps >= 50:
+                break
+    dt = time.perf_counter() - t0
+    rate = n * cfg.substep_iterations * steps / dt
+    return {"value": rate, "unit": METRIC, "cores": cores, "kind": kind,
+            "sample": f"{sample}, {steps} steps in {dt:.1f} s, OpenMP over {cores} host threads"}
+
+
+def run_reference(args, dist):
+    if dist.rank != 0:
+        return
+    cb = cpu_reference_rate(args.cpu_seconds)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload(args.workload)[4] if args.workload == "c0" else
+                       "dam break 4,194,304 particles (timed on a 64^3 sub-block on the host)"},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---- GPU arm ------------------------------------------------------------------------------------------
+def run_b200(args, dist):
+    import torch
+
+    import pbf_b200 as P
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    cfg, pos, vel, sdf, desc = workload(args.workload)
+    n = len(pos)
+    fl = P.PBFluids(cfg, device=dev)
+    fl.setParticles(P.make_particles(pos, vel))
+    obstacle = None
+    if sdf is not None:
+        grid, origin, cell, pad = sdf
+        obstacle = P.GridSDF(grid, origin, cell, device=dev)
+        fl.setSDFBoundary(obstacle)
+        fl.setSDFPadding(pad)
+        fl.setSDFContainment(False)
+    stream = torch.cuda.ExternalStream(fl.stream(), device=dev)
+    for _ in range(args.warmup):
+        fl.step()
+    fl.sync()
+    fl.set_profiling(True)
+    fl.reset_pass_times()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks = Clocks(dev)
+    l0 = fl.kernel_launches()
+    e0.record(stream)
+    for _ in range(args.steps):
+        fl.step()
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+    clk = clocks.stop()
+    launches = fl.kernel_launches() - l0
+    ms = e0.elapsed_time(e1)
+    passes = fl.pass_times()
+    fl.set_profiling(False)
+    bad = fl.check_finite()
+    ms_max = dist.max(ms)
+    subs = cfg.substep_iterations
+    value = n * subs * args.steps * dist.world / (ms_max / 1e3)
+
+    # e2e through the public API with host buffers: upload the state from
+    # pinned memory, step, read the result back, every step
+    pinned = torch.empty(n * 48, dtype=torch.uint8, pin_memory=True)
+    host = pinned.numpy().view(P.PARTICLE_DTYPE)
+    fl.readbackParticles(host)
+    dist.barrier()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        fl.uploadParticles(host)
+        fl.step()
+        fl.readbackParticles(host)
+    e2e_s = dist.max(time.perf_counter() - t0)
+    e2e = {"value": n * subs * args.e2e_steps * dist.world / e2e_s, "unit": METRIC,
+           "h2d_bytes_per_step": n * 48, "d2h_bytes_per_step": n * 48}
+
+    # roofline of the dominant kernel (largest share of device time)
+    pk = peaks()
+    hbm = float(pk.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in pk else "fallback"
+    per_pass = {}
+    for name, (pms, cnt) in passes.items():
+        if name == "step" or cnt == 0:
+            continue
+        per_launch = pms / cnt
+        b = ALGO_BYTES.get(name, 0) * n
+        per_pass[name] = {"ms_total": round(pms, 4), "launches": int(cnt), "ms_per_launch": round(per_launch, 5),
+                          "share": round(pms / max(sum(v[0] for k, v in passes.items() if k != "step"), 1e-9), 4),
+                          "algo_bytes_per_launch": b,
+                          "gbs": round(b / (per_launch / 1e3) / 1e9, 1) if per_launch > 0 else None}
+    dom = max(per_pass, key=lambda k: per_pass[k]["ms_total"]) if per_pass else None
+    tr = traffic_summary().get(dom) if dom else None
+    roof = None
+    if dom:
+        ach = per_pass[dom]["gbs"]
+        roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
+                "frac": round(ach / hbm, 4) if ach else None,
+                "traffic": (int(tr["bytes_per_particle"] * n) if tr else None),
+                "peak_source": peak_src,
+                "note": "neighbour passes are FP32-issue / L1 bound; algorithmic bytes = inputs + outputs once"}
+    cb = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        cb = cpu_reference_rate(args.cpu_seconds)
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": dist.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": desc, "particles_per_gpu": n, "substeps": subs,
+                       "solver_iterations": cfg.solver_iterations, "hash_size": cfg.hash_size,
+                       "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU",
+                       "l2": "working set >> 126 MB L2 (no flush needed)"},
+            "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
+            "passes": per_pass, "nonfinite_particles": int(bad), "impl": "b200"}
+    if dist.rank == 0:
+        print(json.dumps(line), flush=True)
+    del obstacle
+
+
+def main():
+    args = parse()
+    dist = Dist(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference(args, dist)
+        else:
+            run_b200(args, dist)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

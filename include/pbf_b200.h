@@ -1,0 +1,280 @@
+/*
+ * pbf_b200.h — C ABI of the B200 (sm_100a) position-based-fluids substep engine.
+ *
+ * This is the drop-in boundary for the fluid-solver hot path of
+ * enderenest/Realtime-FSI-Engine.  The reference exposes that path only as the
+ * C++ class `PBFluids` (include/fluid/PBFluids.h:191-371) plus the
+ * `SDFBoundary` obstacle (include/fluid/SDFBoundary.h:38-167) and the
+ * fluid-to-mesh contact reduction in src/main.cpp:604-710.  Every entry point
+ * below names the reference member or function it replaces.  The C++ classes
+ * in include/fluid/ (PBFluids.h, SDFBoundary.h) are thin wrappers over these functions.
+ *
+ * Conventions
+ *   - Every function returns an int status: PBF_OK (0) or a negative PBF_ERR_*.
+ *     pbf_last_error() returns a text description of the last failure on the
+ *     calling thread.  No C++ exception crosses this boundary.
+ *   - A handle owns one CUDA stream and all device buffers of one scene.  A
+ *     handle is not thread-safe; distinct handles are independent.
+ *   - Host pointers are plain host memory (pageable or pinned).  Sizes are in
+ *     elements unless a name ends in _bytes.
+ *   - pbf_step() is asynchronous on the handle's stream; every pbf_read_*()
+ *     synchronizes the stream before it returns.
+ */
+#ifndef PBF_B200_H
+#define PBF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PBF_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------- */
+#define PBF_OK 0
+#define PBF_ERR_INVALID -1   /* bad argument (null pointer, size, range)       */
+#define PBF_ERR_CUDA -2      /* a CUDA runtime call failed                      */
+#define PBF_ERR_STATE -3     /* call not valid in the current handle state      */
+#define PBF_ERR_ALLOC -4     /* device or host allocation failed               */
+#define PBF_ERR_NUMERIC -5   /* NaN/Inf detected in particle state             */
+#define PBF_ERR_TIMEOUT -6   /* a bounded device-side wait gave up             */
+#define PBF_ERR_NOT_BUILT -7 /* feature compiled out / library missing          */
+
+/* ---- plain-C mirrors of the reference's POD types ------------------------ */
+
+/* FluidConfig (include/core/config.h:9-63).  Field order, meaning and the
+ * defaults filled in by pbf_default_config() follow the reference struct;
+ * booleans are uint32_t (0/1) so the layout is fixed for every FFI. */
+typedef struct pbf_fluid_config {
+    float dt;                  /* macro time step                               */
+    float gravity[3];
+    float h;                   /* smoothing radius                              */
+    float rho0;                /* rest density (unit particle mass implied)     */
+    uint32_t solver_iterations;
+    uint32_t substep_iterations;
+    float eps;                 /* CFM relaxation epsilon                        */
+    uint32_t particle_count;
+    float spawn_min[3];
+    float spawn_max[3];
+    uint32_t spawn_random;
+    float spacing;
+    float initial_velocity[3];
+    float bounds_min[3];
+    float bounds_max[3];
+    float bound_damping;
+    uint32_t hash_size;        /* must be a power of two                        */
+    uint32_t enable_scorr;
+    float k_corr;
+    float n_corr;
+    float delta_q;
+    float cohesion_strength;
+    uint32_t enable_viscosity;
+    float viscosity;
+    float interaction_radius;
+    float interaction_strength;
+    uint32_t enable_vorticity;
+    float vorticity_epsilon;
+    uint32_t enable_apbf;
+    uint32_t min_lod;
+    uint32_t max_lod;
+    float lod_max_dist;
+} pbf_fluid_config;
+
+/* Particle (include/fluid/Particle.h:8-12): three vec3 each padded to 16 B. */
+typedef struct pbf_particle {
+    float pos[3];
+    float pad0;
+    float pred_pos[3];
+    float pad1;
+    float vel[3];
+    float pad2;
+} pbf_particle;
+
+/* ContactCandidate (include/fluid/PBFluids.h:67-70). */
+typedef struct pbf_contact_candidate {
+    float pos[4]; /* xyz world position, w unused */
+    float vel[4]; /* xyz velocity, w unused       */
+} pbf_contact_candidate;
+
+/* Derived solver constants: the FluidConfigUBO block of
+ * include/fluid/PBFluids.h:21-61 as PBFluids::setParams
+ * (src/fluid/PBFluids.cpp:39-109) fills it. */
+typedef struct pbf_derived_params {
+    float bounds_min[4];
+    float bounds_max[4];
+    float gravity_dt[4]; /* xyz gravity, w substep dt */
+    float h, rho0, eps, wq;
+    float k_corr, n_corr, viscosity, bound_damping;
+    uint32_t hash_size, particle_count, enable_scorr, enable_viscosity;
+    float cohesion_strength, interaction_radius, interaction_strength, w0_self;
+    uint32_t hash_mask;
+    float poly6_coeff, spiky_coeff, inv_rho0;
+    uint32_t min_lod, max_lod;
+    float lod_max_dist;
+    uint32_t enable_apbf;
+} pbf_derived_params;
+
+typedef struct pbf_handle pbf_handle;
+
+/* ---- library ------------------------------------------------------------ */
+int pbf_abi_version(void);
+const char* pbf_last_error(void);
+/* FluidConfig's in-class defaults (include/core/config.h:11-62). */
+int pbf_default_config(pbf_fluid_config* out);
+/* Host-side setParams derivation (src/fluid/PBFluids.cpp:39-109), exposed so
+ * callers and tests see exactly the constants the kernels use.  `collision_padding`
+ * is PBFluids::_collisionPadding (include/fluid/PBFluids.h:108-109). */
+int pbf_derive_params(const pbf_fluid_config* cfg, float collision_padding,
+                      pbf_derived_params* out);
+
+/* ---- lifecycle (PBFluids::PBFluids / ~PBFluids, src/fluid/PBFluids.cpp:12-37) */
+int pbf_create(const pbf_fluid_config* cfg, int device, pbf_handle** out);
+int pbf_destroy(pbf_handle* h);
+
+/* ---- parameters (PBFluids::setParams / setBounds / setCollisionPadding /
+ *      setCameraPos / setInteraction, PBFluids.h:93-135, PBFluids.cpp:39-109,
+ *      299-317) */
+int pbf_set_params(pbf_handle* h, const pbf_fluid_config* cfg);
+int pbf_get_params(pbf_handle* h, pbf_fluid_config* out);
+int pbf_get_derived(pbf_handle* h, pbf_derived_params* out);
+int pbf_set_bounds(pbf_handle* h, const float min_bound[3], const float max_bound[3],
+                   float damping);
+int pbf_set_collision_padding(pbf_handle* h, float padding);
+int pbf_set_camera_pos(pbf_handle* h, const float pos[3]);
+int pbf_set_interaction(pbf_handle* h, int active, const float pos[3]);
+
+/* ---- particles (PBFluids::setParticles / readbackParticles,
+ *      PBFluids.cpp:111-191).  n == 0 clears the scene (step() then no-ops,
+ *      as PBFluids.cpp:325). */
+int pbf_set_particles(pbf_handle* h, const pbf_particle* particles, uint32_t n);
+/* Refresh the state of an unchanged particle count from host memory
+ * (asynchronous on the handle's stream; pinned memory makes it a DMA).
+ * No reference counterpart: setParticles also reallocates and re-derives. */
+int pbf_upload_particles(pbf_handle* h, const pbf_particle* particles, uint32_t n);
+int pbf_particle_count(pbf_handle* h, uint32_t* n);
+int pbf_read_particles(pbf_handle* h, pbf_particle* out, uint32_t n);
+/* Device-resident particle upload/download in the engine's own layout:
+ * pos4 and vel4 are n float4 (xyz, w ignored) device pointers. */
+int pbf_set_particles_device(pbf_handle* h, const void* pos4_dev, const void* vel4_dev,
+                             uint32_t n);
+int pbf_read_particles_device(pbf_handle* h, void* pos4_dev, void* vel4_dev, uint32_t n);
+
+/* ---- stepping (PBFluids::step, PBFluids.cpp:323-517) ---------------------- */
+int pbf_step(pbf_handle* h);
+int pbf_sync(pbf_handle* h);
+/* Raw cudaStream_t of the handle (for event timing / interop). */
+int pbf_get_stream(pbf_handle* h, void** stream);
+
+/* ---- SDF obstacle (PBFluids::setSDFBoundary / setSDFPadding /
+ *      setSDFContainment, PBFluids.h:117-129; the sampled grid replaces
+ *      SDFBoundary::uploadToGPU + Texture3D, SDFBoundary.cpp:580-598).
+ *      `dist` is in the reference CPU order index(x,y,z) = x*dy*dz + y*dz + z
+ *      (SDFBoundary.h:111-113); origin is the world position of voxel (0,0,0). */
+int pbf_set_sdf_grid(pbf_handle* h, const float* dist, const int32_t dims[3],
+                     const float origin[3], float cell_size);
+int pbf_clear_sdf(pbf_handle* h);
+/* Collide `h` with the SDF held by another handle `sdf` (same device) without
+ * copying it: the non-owning pointer of PBFluids::setSDFBoundary
+ * (PBFluids.h:117-120).  The caller keeps `sdf` alive while attached and
+ * re-attaches after rebuilding it, as the reference does (main.cpp:852-854).
+ * sdf == NULL detaches. */
+int pbf_attach_sdf(pbf_handle* h, pbf_handle* sdf);
+int pbf_set_sdf_mode(pbf_handle* h, float padding, int containment);
+int pbf_read_sdf_grid(pbf_handle* h, float* out, size_t n);
+/* Sample the active SDF at n world points (software trilinear, clamp to edge,
+ * exactly as the step kernels query it).  out_grad may be NULL. */
+int pbf_sample_sdf(pbf_handle* h, const float* pts3, uint32_t n, float* out_d,
+                   float* out_grad3);
+
+/* ---- triangle-mesh SDF (SDFBoundary::buildFromMesh / refitFromMesh /
+ *      closestTriangle, SDFBoundary.cpp:278-465,600-610).  verts: nv*3 doubles,
+ *      faces: nf*3 int32.  The grid is computed on the GPU from an LBVH and
+ *      becomes the active SDF of the handle. */
+int pbf_set_sdf_mesh(pbf_handle* h, const double* verts, int32_t nv, const int32_t* faces,
+                     int32_t nf, double cell_size);
+/* Moved vertices, same topology: GPU LBVH refit + face-normal refresh + full
+ * grid recompute (edge/vertex pseudo-normals keep their build-time values,
+ * SDFBoundary.h:58-62). */
+int pbf_update_mesh_vertices(pbf_handle* h, const double* verts, int32_t nv);
+int pbf_sdf_grid_info(pbf_handle* h, int32_t dims[3], double origin[3], double* cell_size);
+/* Closest point on the mesh for n query points (SDFBoundary::closestTriangle). */
+int pbf_closest_triangle(pbf_handle* h, const float* pts3, uint32_t n, int32_t* out_face,
+                         float* out_point3);
+
+/* ---- contacts (PBFluids::filterContactCandidates / readbackContactCandidates,
+ *      PBFluids.cpp:193-284; computeContactForces, src/main.cpp:604-710) ---- */
+/* Near-surface compaction |sdf(x)| < band, in particle-index order (the
+ * reference appends atomically in arbitrary order; this build is
+ * deterministic).  band <= 0 or no SDF: no-op, as the reference. */
+int pbf_filter_contacts(pbf_handle* h, float band);
+int pbf_read_contacts(pbf_handle* h, pbf_contact_candidate* out, uint32_t capacity,
+                      uint32_t* count);
+/* Per-vertex fluid push forces from the current candidate list against the
+ * current mesh: out3 receives nv*3 floats; out_contacts the number of
+ * contributing candidates.  use_vel_magnitude mirrors g_useVelMagnitude. */
+int pbf_vertex_forces(pbf_handle* h, float band, int use_vel_magnitude, float* out3,
+                      int32_t nv, int32_t* out_contacts);
+
+/* ---- stage-level access for parity tests -------------------------------- */
+enum pbf_stage {
+    PBF_STAGE_PREDICT = 1,   /* CS_PredictAndHash: keys (+ x*, v' recomputed later) */
+    PBF_STAGE_SORT = 2,      /* CS_Radix*: stable sort of (key, id)                 */
+    PBF_STAGE_TABLE = 3,     /* CS_BuildOffsets: clear + build the hash-cell table  */
+    PBF_STAGE_REORDER = 4,   /* gather x*, v', x into sorted float4 SoA (+ LOD)     */
+    PBF_STAGE_LAMBDA = 5,    /* CS_ComputeLambdas (iteration `iter`, 1-based)       */
+    PBF_STAGE_DELTAP = 6,    /* CS_ComputeDeltaP + CS_ApplyDeltaP fused             */
+    PBF_STAGE_INTEGRATE = 7, /* CS_Integrate                                         */
+    PBF_STAGE_VORTICITY = 8  /* CS_VorticityConfinement pass 1                       */
+};
+int pbf_run_stage(pbf_handle* h, int stage, uint32_t iter);
+
+enum pbf_buffer {
+    PBF_BUF_KEYS = 1,        /* uint32[N]  unsorted hash keys (particle order)      */
+    PBF_BUF_SORTED_KEYS = 2, /* uint32[N]  sorted keys                              */
+    PBF_BUF_SORTED_IDS = 3,  /* uint32[N]  particle id of each sorted slot          */
+    PBF_BUF_TABLE = 4,       /* int32[2H]  (start, end) per hash, -1 if empty       */
+    PBF_BUF_XSTAR = 5,       /* float4[N]  current (x*, lambda) in sorted order     */
+    PBF_BUF_VPRED = 6,       /* float4[N]  post-predict velocity, sorted order      */
+    PBF_BUF_RHO = 7,         /* float[N]   density of the last lambda pass, sorted  */
+    PBF_BUF_OMEGA = 8,       /* float4[N]  curl omega of the last integrate, sorted */
+    PBF_BUF_POS = 9,         /* float4[N]  committed positions, particle order      */
+    PBF_BUF_VEL = 10,        /* float4[N]  committed velocities, particle order     */
+    PBF_BUF_LOD = 11         /* uint32[N]  APBF level per sorted slot               */
+};
+int pbf_read_buffer(pbf_handle* h, int which, void* out, size_t bytes);
+int pbf_buffer_device_ptr(pbf_handle* h, int which, void** dev_ptr, size_t* bytes);
+
+/* ---- standalone primitives (host buffers in, host buffers out) ---------- */
+/* Stable LSD radix sort of n keys < 2^key_bits with ids 0..n-1 — the contract
+ * of the CS_RadixHistogram/PrefixSum/Scatter chain (PBFluids.cpp:354-405). */
+int pbf_sort_keys(const uint32_t* keys, uint32_t n, uint32_t key_bits,
+                  uint32_t* sorted_keys, uint32_t* sorted_ids);
+/* CS_BuildOffsets (clear + build) over sorted keys into table[2*hash_size]. */
+int pbf_build_table(const uint32_t* sorted_keys, uint32_t n, uint32_t hash_size,
+                    int32_t* table);
+
+/* ---- timing ------------------------------------------------------------- */
+/* When on, every pass of pbf_step records CUDA events on the handle's stream
+ * and accumulates per-pass device time (read with pbf_read_pass_times).
+ * Pass slots follow enum pbf_stage (index = stage); slot 0 = whole steps. */
+#define PBF_NUM_PASS_SLOTS 12
+int pbf_set_profiling(pbf_handle* h, int on);
+int pbf_read_pass_times(pbf_handle* h, double* ms_out, uint64_t* launches_out);
+int pbf_reset_pass_times(pbf_handle* h);
+/* Number of kernels this library launched on the handle since creation. */
+int pbf_kernel_launches(pbf_handle* h, uint64_t* out);
+/* CUDA-graph replay of one full step (captured lazily, invalidated by any
+ * parameter, particle or SDF change). */
+int pbf_set_use_graph(pbf_handle* h, int on);
+
+/* ---- health ------------------------------------------------------------- */
+/* Scan committed state for NaN/Inf; *bad receives the count (0 = healthy). */
+int pbf_check_finite(pbf_handle* h, uint32_t* bad);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* PBF_B200_H */

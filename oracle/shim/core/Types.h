@@ -1,0 +1,35 @@
+/*
+ * Eigen-free stand-in for the reference's include/core/Types.h, used only to
+ * compile the reference's own CPU files src/fluid/Kernels.cpp and
+ * src/fluid/NeighborSearch.cpp under oracle/_ref.  It declares the plain
+ * fluid types those files use (the "Fluid (GPU) - Plain Vectors" half of
+ * include/core/Types.h:37-77) with the same names, because the reference
+ * sources refer to them by those names; the Eigen/CHOLMOD half is omitted
+ * (Eigen/Core is absent from the reference's vendored tree).
+ */
+#ifndef TYPES_H
+#define TYPES_H
+#include <cmath>
+#include <cstdint>
+
+using F32 = float;
+using I32 = std::int32_t;
+using U32 = std::uint32_t;
+
+struct PVec3 { F32 x, y, z; };
+struct PVec4 { F32 x, y, z, w; };
+struct UVec2 { U32 x, y; };
+struct IVec2 { I32 x, y; };
+
+inline PVec3 make_pvec3(F32 x, F32 y, F32 z) { return PVec3{x, y, z}; }
+inline PVec3 operator+(PVec3 a, PVec3 b) { return PVec3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline PVec3 operator-(PVec3 a, PVec3 b) { return PVec3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline PVec3 operator*(PVec3 a, F32 s) { return PVec3{a.x * s, a.y * s, a.z * s}; }
+inline PVec3 operator*(F32 s, PVec3 a) { return a * s; }
+inline PVec3& operator+=(PVec3& a, PVec3 b) { a = a + b; return a; }
+inline PVec3& operator-=(PVec3& a, PVec3 b) { a = a - b; return a; }
+inline PVec3& operator*=(PVec3& a, F32 s) { a = a * s; return a; }
+inline F32 dot(PVec3 a, PVec3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline F32 norm2(PVec3 a) { return dot(a, a); }
+inline F32 norm(PVec3 a) { return std::sqrt(norm2(a)); }
+#endif

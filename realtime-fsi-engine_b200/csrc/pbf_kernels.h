@@ -1,0 +1,74 @@
+// pbf_kernels.h — host-side launchers of the engine's kernels.
+#pragma once
+
+#include "pbf_internal.cuh"
+
+namespace pbf {
+
+// ---- k_solver.cu ------------------------------------------------------------
+void launch_predict_hash(const DevParams& P, const float4* pos, const float4* vel, uint32_t* keys, int sms,
+                         cudaStream_t st);
+void launch_reorder(const DevParams& P, const uint32_t* ids, const float4* pos, const float4* vel, float4* sx,
+                    float4* sv, float4* sx0, uint32_t* lod, int sms, cudaStream_t st);
+void launch_build_table(uint32_t n, const uint32_t* sk, int2* table, int sms, cudaStream_t st);
+void launch_lambda(const DevParams& P, const float4* xin, float4* xout, float* rho, const int2* table,
+                   const uint32_t* lod, uint32_t iter, cudaStream_t st);
+void launch_deltap_apply(const DevParams& P, const float4* xin, float4* xout, const int2* table,
+                         const uint32_t* lod, uint32_t iter, cudaStream_t st);
+void launch_integrate(const DevParams& P, const float4* xs, const float4* sv, float4* sx0, float4* somega,
+                      const uint32_t* ids, float4* pos, float4* vel, const int2* table, cudaStream_t st);
+void launch_vorticity(const DevParams& P, const float4* spos, const float4* somega, const uint32_t* ids,
+                      float4* vel, const int2* table, cudaStream_t st);
+void launch_check_finite(uint32_t n, const float4* pos, const float4* vel, uint32_t* bad, int sms,
+                         cudaStream_t st);
+void launch_unpack_particles(uint32_t n, const float4* aos, float4* pos, float4* pred, float4* vel, int sms,
+                             cudaStream_t st);
+void launch_pack_particles(uint32_t n, const float4* pos, const float4* pred, const float4* vel, float4* aos,
+                           int sms, cudaStream_t st);
+
+// ---- k_sort.cu ----------------------------------------------------------------
+uint32_t sort_num_tiles(uint32_t n);
+void launch_radix_sort(uint32_t n, uint32_t key_bits, const uint32_t* keys_in, uint32_t* ka, uint32_t* ia,
+                       uint32_t* kb, uint32_t* ib, uint32_t* hist, uint32_t* totals, uint32_t** out_keys,
+                       uint32_t** out_ids, cudaStream_t st, uint64_t* launches);
+
+// ---- k_sdf.cu -----------------------------------------------------------------
+void launch_sdf_slab_min(const float* dist, int dx, int dy, int dz, float* slab_min, cudaStream_t st);
+void launch_sdf_sample(SdfDev S, const float* pts3, uint32_t n, float* d, float* grad3, cudaStream_t st);
+// Contact compaction |sdf(pos)| < band in particle order.  Scratch: counts of
+// contact_num_blocks(n) uint32 and one uint32 total.
+uint32_t contact_num_blocks(uint32_t n);
+void launch_contact_filter(SdfDev S, uint32_t n, const float4* pos, const float4* vel, float band,
+                           uint32_t* block_counts, uint32_t* total, float4* out_cand, cudaStream_t st,
+                           uint64_t* launches);
+
+// ---- k_mesh.cu ------------------------------------------------------------------
+struct MeshDev {
+    int nv, nf;
+    const int3* faces;    // nf
+    float3* verts;        // nv, current positions
+    float3* face_n;       // nf, refreshed on refit
+    const float3* edge_n; // nf*3 (AB, AC, BC), build-time
+    const float3* vert_n; // nv, build-time
+    // LBVH over the faces (Karras 2012): nf leaves, nf-1 internal nodes
+    int2* child;          // internal child indices; >= nf-1 + leaf marks leaves (encoded)
+    int* parent;          // 2nf-1
+    float4* bmin;         // 2nf-1 (xyz)
+    float4* bmax;         // 2nf-1
+    int* leaf_face;       // nf: face index of leaf i (Morton order)
+    uint32_t* flags;      // nf-1 refit arrival counters
+};
+void launch_mesh_refit(MeshDev M, cudaStream_t st, uint64_t* launches);
+void launch_mesh_grid_d(MeshDev M, int dx, int dy, int dz, const double* origin, double cell, float* out, int sms,
+                        cudaStream_t st);
+void launch_morton(int nf, const int3* faces, const float3* verts, float3 lo, float3 inv_ext, uint32_t* codes,
+                   cudaStream_t st);
+void launch_mesh_closest(MeshDev M, const float* pts3, uint32_t n, int* face, float* point3, cudaStream_t st);
+// Per-vertex force accumulation in 2^-32 fixed point (deterministic).
+void launch_vertex_forces(MeshDev M, const float4* cand, const uint32_t* count, uint32_t cap, float band,
+                          int use_vel, long long* acc3, int* contacts, cudaStream_t st);
+void launch_forces_to_float(int nv, const long long* acc3, float* out3, cudaStream_t st);
+// LBVH topology from sorted Morton codes (device).
+void launch_lbvh_topology(int nf, const uint32_t* sorted_codes, int2* child, int* parent, cudaStream_t st);
+
+}  // namespace pbf

@@ -1,0 +1,285 @@
+"""Parity of the sm_100a kernels (through the C ABI) with the FP64 oracle.
+
+Integer work (hash keys, the stable sort permutation, the cell table, contact
+compaction) must be bit-exact.  Floating-point stages are fed identical inputs
+(the GPU's own state, converted to FP64) and must agree within FP32 rounding:
+positions within 1e-5*h, other quantities relative to their scale as stated
+in each assert.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle as O
+import pbf_b200 as P
+import pbfh as H
+from pbf_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+STAGE_FIXTURES = ["glsl_stages_plain.npz", "glsl_stages_scorr.npz", "glsl_stages_sdf.npz",
+                  "glsl_stages_container.npz", "glsl_stages_apbf.npz"]
+
+
+def make_fluid(z):
+    cfg = H.engine_cfg(z)
+    fl = P.PBFluids(cfg)
+    fl.setParticles(P.make_particles(z["pos0"], z["vel0"]))
+    if "camera" in z:
+        fl.setCameraPos(z["camera"])
+    if "interaction" in z:
+        fl.setInteraction(True, z["interaction"])
+    sdf = None
+    if "sdf_dist" in z:
+        sdf = P.GridSDF(z["sdf_dist"], z["sdf_origin"], float(z["sdf_cell"]))
+        fl.setSDFBoundary(sdf)
+        fl.setSDFPadding(float(z["sdf_padding"]))
+        fl.setSDFContainment(bool(z["sdf_containment"]))
+    return fl, sdf
+
+
+def gpu_sorted(fl, n):
+    ids = fl.read_buffer(P.BUF_SORTED_IDS, np.uint32, n)
+    xs = fl.read_buffer(P.BUF_XSTAR, np.float32, (n, 4))
+    orig = np.zeros_like(xs)
+    orig[ids] = xs
+    return ids, xs, orig
+
+
+# ---- sort / table -----------------------------------------------------------------
+@pytest.mark.parametrize("n,bits,dist", [
+    (1, 8, "rand"), (255, 8, "rand"), (4096, 17, "rand"), (4097, 17, "rand"), (100003, 22, "rand"),
+    (1 << 20, 22, "rand"), (50000, 17, "equal"), (50000, 17, "sorted"), (50000, 17, "reverse"),
+    (70001, 30, "few"), (20000, 32, "rand"), (30000, 1, "rand"), (9999, 9, "rand"),
+])
+def test_radix_sort_is_stable_and_bit_exact(have_gpu, n, bits, dist):
+    rng = np.random.default_rng(n + bits)
+    hi = (1 << bits) if bits < 32 else (1 << 32)
+    if dist == "rand":
+        keys = rng.integers(0, hi, size=n, dtype=np.uint64).astype(np.uint32)
+    elif dist == "equal":
+        keys = np.full(n, hi - 1, np.uint32)
+    elif dist == "sorted":
+        keys = np.sort(rng.integers(0, hi, size=n)).astype(np.uint32)
+    elif dist == "reverse":
+        keys = np.sort(rng.integers(0, hi, size=n))[::-1].astype(np.uint32)
+    else:
+        keys = rng.choice(np.array([0, 7, hi - 1, 12345 % hi], np.uint64), size=n).astype(np.uint32)
+    sk, ids = P.sort_keys(keys, bits)
+    order = np.argsort(keys, kind="stable")
+    assert np.array_equal(ids, order.astype(np.uint32))
+    assert np.array_equal(sk, keys[order])
+
+
+def test_cell_table_bit_exact(have_gpu):
+    rng = np.random.default_rng(5)
+    for n, H_ in [(0, 1024), (1, 16), (5000, 1 << 12), (300000, 1 << 18)]:
+        sk = np.sort(rng.integers(0, H_, size=n)).astype(np.uint32)
+        t = P.build_table(sk, H_)
+        ref = O.build_table(sk, H_) if n else np.full((H_, 2), -1, np.int32)
+        assert np.array_equal(t, ref)
+        assert (t[:, 1] - t[:, 0])[t[:, 0] >= 0].sum() == n
+
+
+# ---- substep stages against the oracle (GPU inputs -> FP64) ---------------------------
+@pytest.mark.parametrize("name", STAGE_FIXTURES)
+def test_stages_match_oracle(have_gpu, name):
+    z = H.load(name)
+    fl, sdf = make_fluid(z)
+    p = H.oracle_params(z)
+    S = H.oracle_sdf(z)
+    L = O.lib()
+    n = len(z["pos0"])
+    h = p.cfg.h
+    for st in (P.STAGE_PREDICT, P.STAGE_SORT, P.STAGE_TABLE, P.STAGE_REORDER):
+        fl.run_stage(st)
+    keys = fl.read_buffer(P.BUF_KEYS, np.uint32, n)
+    sk = fl.read_buffer(P.BUF_SORTED_KEYS, np.uint32, n)
+    table = fl.read_buffer(P.BUF_TABLE, np.int32, (p.cfg.hash_size, 2))
+    ids, xs, xs_orig = gpu_sorted(fl, n)
+    # keys from the GPU's own FP32 x*, its permutation and table: bit-exact
+    assert np.array_equal(keys, O.keys_f32(xs_orig, h, p.cfg.hash_size - 1))
+    osk, oids = O.stable_sort(keys, p.cfg.hash_size)
+    assert np.array_equal(sk, osk) and np.array_equal(ids, oids)
+    assert np.array_equal(table, O.build_table(osk, p.cfg.hash_size))
+    # x* and v' against FP64 predict
+    pos, vel = H.f64(z["pos0"]), H.f64(z["vel0"]).copy()
+    x64 = np.zeros((n, 3))
+    L.orc_predict(C.byref(p.p), n, pos.reshape(-1), vel.reshape(-1), x64.reshape(-1), None)
+    assert np.abs(xs_orig[:, :3] - x64).max() < 1e-5 * h
+    sv = fl.read_buffer(P.BUF_VPRED, np.float32, (n, 4))
+    v_orig = np.zeros_like(sv)
+    v_orig[ids] = sv
+    assert np.abs(v_orig[:, :3] - vel).max() < 1e-6 * max(1.0, np.abs(vel).max())
+    lod = None
+    if p.p.apbf:
+        lod_s = fl.read_buffer(P.BUF_LOD, np.uint32, n)
+        lod = np.zeros(n, np.uint32)
+        lod[ids] = lod_s
+        olod = np.zeros(n, np.uint32)
+        L.orc_lod(C.byref(p.p), n, H.f64(xs_orig[:, :3]).reshape(-1), olod)
+        assert np.array_equal(lod, olod)
+    lodp = lod.ctypes.data_as(C.c_void_p) if lod is not None else None
+    iters = p.p.max_lod if p.p.apbf else p.cfg.solver_iterations
+    tabf = table.reshape(-1)
+    for it in range(1, iters + 1):
+        _, _, x_in = gpu_sorted(fl, n)
+        fl.run_stage(P.STAGE_LAMBDA, it)
+        _, xl, xl_orig = gpu_sorted(fl, n)
+        lam = np.zeros(n)
+        rho = np.zeros(n)
+        lam[:] = x_in[:, 3]  # inactive APBF particles keep their lambda
+        L.orc_lambda(C.byref(p.p), n, H.f64(x_in[:, :3]).reshape(-1), ids, tabf, lodp, it, lam,
+                     rho.ctypes.data_as(C.c_void_p))
+        assert np.abs(xl_orig[:, 3] - lam).max() <= 2e-5 * np.abs(lam).max() + 1e-12, it
+        rho_g = np.zeros(n, np.float32)
+        rho_g[ids] = fl.read_buffer(P.BUF_RHO, np.float32, n)
+        act = np.ones(n, bool) if lod is None else lod >= it
+        assert np.abs(rho_g - rho)[act].max() < 2e-6 * rho.max()
+        fl.run_stage(P.STAGE_DELTAP, it)
+        _, _, xd_orig = gpu_sorted(fl, n)
+        x64 = H.f64(xl_orig[:, :3]).copy()
+        L.orc_deltap_apply(C.byref(p.p), S.ref() if S else None, n, x64.reshape(-1), H.f64(xl_orig[:, 3]), ids,
+                           tabf, lodp, it, None)
+        assert np.abs(xd_orig[:, :3] - x64).max() < 1e-5 * h, it
+    # integrate
+    _, _, xf_orig = gpu_sorted(fl, n)
+    fl.run_stage(P.STAGE_INTEGRATE)
+    pos_g = fl.read_buffer(P.BUF_POS, np.float32, (n, 4))
+    vel_g = fl.read_buffer(P.BUF_VEL, np.float32, (n, 4))
+    om_g = np.zeros((n, 4), np.float32)
+    om_g[ids] = fl.read_buffer(P.BUF_OMEGA, np.float32, (n, 4))
+    p64, v64, om = H.f64(z["pos0"]).copy(), H.f64(v_orig[:, :3]).copy(), np.zeros((n, 3))
+    L.orc_integrate(C.byref(p.p), S.ref() if S else None, n, p64.reshape(-1), v64.reshape(-1),
+                    H.f64(xf_orig[:, :3]).reshape(-1), ids, tabf, om.ctypes.data_as(C.c_void_p))
+    assert np.abs(pos_g[:, :3] - p64).max() < 1e-5 * h
+    assert np.abs(om_g[:, :3] - om).max() < 2e-5 * max(np.abs(om).max(), 1e-9)
+    keep = np.ones(n, bool)
+    if S is not None:
+        xc = np.clip(H.f64(xf_orig[:, :3]), np.array(p.p.bmin[:]), np.array(p.p.bmax[:]))
+        d, _ = S.query(xc)
+        thr = -S.s.padding if S.s.containment else S.s.padding
+        keep = np.abs(d - thr) > 1e-5 * S.s.cell
+    vs = max(np.abs(v64).max(), 1.0)
+    assert np.abs(vel_g[:, :3] - v64)[keep].max() < 2e-5 * vs
+    # vorticity
+    fl.run_stage(P.STAGE_VORTICITY)
+    vel2 = fl.read_buffer(P.BUF_VEL, np.float32, (n, 4))
+    v3 = H.f64(vel_g[:, :3]).copy()
+    L.orc_vorticity(C.byref(p.p), n, H.f64(pos_g[:, :3]).reshape(-1), v3.reshape(-1), H.f64(om_g[:, :3]).reshape(-1),
+                    ids, tabf)
+    assert np.abs(vel2[:, :3] - v3).max() < 1e-5 * vs
+
+
+@pytest.mark.parametrize("name", ["glsl_stages_plain.npz", "glsl_stages_apbf.npz"])
+def test_first_substep_matches_reference_shaders_directly(have_gpu, name):
+    """GPU substep vs the reference's own FP32 shader result (golden)."""
+    z = H.load(name)
+    fl, _ = make_fluid(z)
+    n = len(z["pos0"])
+    for st in (P.STAGE_PREDICT, P.STAGE_SORT, P.STAGE_TABLE, P.STAGE_REORDER):
+        fl.run_stage(st)
+    assert np.array_equal(fl.read_buffer(P.BUF_KEYS, np.uint32, n), z["pred_keys"])
+    assert np.array_equal(fl.read_buffer(P.BUF_SORTED_IDS, np.uint32, n), z["sorted_grid"][:, 1])
+    assert np.array_equal(fl.read_buffer(P.BUF_TABLE, np.int32, z["offsets"].shape), z["offsets"])
+    cfg = H.engine_cfg(z)
+    iters = cfg.max_lod if cfg.enable_apbf else cfg.solver_iterations
+    for it in range(1, iters + 1):
+        fl.run_stage(P.STAGE_LAMBDA, it)
+        fl.run_stage(P.STAGE_DELTAP, it)
+    fl.run_stage(P.STAGE_INTEGRATE)
+    pos = fl.read_buffer(P.BUF_POS, np.float32, (n, 4))[:, :3]
+    assert np.abs(pos - z["int_pos"]).max() < 1e-5 * cfg.h
+
+
+def test_full_step_matches_oracle_smooth_regime(have_gpu):
+    cfg, pos, vel = scenes.c0(16, seed=2)
+    cfg.enable_scorr = 0
+    cfg.particle_count = len(pos)
+    vel = np.random.default_rng(9).uniform(-0.2, 0.2, pos.shape).astype(np.float32)
+    fl = P.PBFluids(cfg)
+    fl.setParticles(P.make_particles(pos, vel))
+    fl.step()
+    out = fl.readbackParticles()
+    ocfg = O.FluidConfig()
+    C.memmove(C.byref(ocfg), C.byref(cfg), C.sizeof(ocfg))
+    p = O.Params(ocfg)
+    p64, v64 = H.f64(pos).copy(), H.f64(vel).copy()
+    O.step(p, p64, v64)
+    err = np.abs(out["pos"] - p64).max()
+    assert err <= 1e-5 * cfg.h, err / cfg.h
+    assert np.abs(out["vel"] - v64).max() < 1e-3
+    # predPos and the pad words come back as uploaded
+    assert np.array_equal(out["pred_pos"], pos)
+
+
+def test_graph_replay_and_repeat_runs_are_bit_identical(have_gpu):
+    cfg, pos, vel = scenes.c0(16, seed=1)
+    runs = []
+    for graph in (False, True, True):
+        fl = P.PBFluids(cfg)
+        fl.setParticles(P.make_particles(pos, vel))
+        fl.set_use_graph(graph)
+        for _ in range(3):
+            fl.step()
+        runs.append(fl.readbackParticles())
+        assert fl.kernel_launches() > 0
+    for r in runs[1:]:
+        assert np.array_equal(r["pos"], runs[0]["pos"]) and np.array_equal(r["vel"], runs[0]["vel"])
+
+
+def test_empty_scene_and_errors(have_gpu):
+    cfg, pos, vel = scenes.c0(8)
+    fl = P.PBFluids(cfg)
+    fl.setParticles(P.make_particles(pos[:0]))
+    fl.step()  # no-op, as PBFluids.cpp:325
+    assert len(fl.readbackParticles()) == 0
+    with pytest.raises(P.PBFError):
+        fl.run_stage(P.STAGE_LAMBDA, 1)
+    fl.setParticles(P.make_particles(pos, vel))
+    with pytest.raises(P.PBFError):
+        fl.run_stage(P.STAGE_LAMBDA, 1)  # before the sort
+    buf = np.zeros(3, P.PARTICLE_DTYPE)
+    from pbf_b200 import _capi
+    assert _capi.lib().pbf_read_particles(fl.handle, buf.ctypes.data_as(C.c_void_p), 3) == _capi.PBF_ERR_INVALID
+    fl.step()
+    assert fl.check_finite() == 0
+
+
+# ---- SDF grid and contacts ---------------------------------------------------------------
+def test_sdf_sampling_matches_oracle(have_gpu):
+    z = H.load("glsl_stages_sdf.npz")
+    g = P.GridSDF(z["sdf_dist"], z["sdf_origin"], float(z["sdf_cell"]))
+    S = H.oracle_sdf(z)
+    rng = np.random.default_rng(3)
+    lo = np.array(z["sdf_origin"]) - 0.05
+    hi = lo + np.array(z["sdf_dist"].shape) * float(z["sdf_cell"]) + 0.1
+    pts = rng.uniform(lo, hi, size=(4000, 3)).astype(np.float32)
+    d = np.empty(len(pts), np.float32)
+    gr = np.empty((len(pts), 3), np.float32)
+    from pbf_b200 import _capi
+    _capi.check(_capi.lib().pbf_sample_sdf(g._h, pts.ctypes.data_as(C.c_void_p), len(pts),
+                                           d.ctypes.data_as(C.c_void_p), gr.ctypes.data_as(C.c_void_p)))
+    od, og = S.query(pts)
+    assert np.abs(d - od).max() < 1e-6
+    assert np.abs(gr - og).max() < 1e-3
+
+
+def test_contact_filter_deterministic_and_exact(have_gpu):
+    z = H.load("glsl_contacts.npz")
+    fl, sdf = make_fluid(z)
+    fl.filterContactCandidates(float(z["band"]))
+    got = fl.readbackContactCandidates()
+    S = H.oracle_sdf(z)
+    pos = H.f64(z["pos0"])
+    idx = np.zeros(len(pos), np.uint32)
+    c = O.lib().orc_contact_filter(S.ref(), len(pos), pos.reshape(-1), float(z["band"]), idx)
+    assert len(got) == c > 0
+    # particle-index order, {pos, 0} and {vel, pad}
+    assert np.array_equal(got["pos"][:, :3], z["pos0"][idx[:c]])
+    assert np.all(got["pos"][:, 3] == 0)
+    assert np.array_equal(got["vel"][:, :3], z["vel0"][idx[:c]])
+    # band <= 0 is a no-op that keeps the previous list (PBFluids.cpp:195)
+    fl.filterContactCandidates(0.0)
+    assert len(fl.readbackContactCandidates()) == c
