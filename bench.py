@@ -46,6 +46,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", type=int, default=1, choices=[0, 1, 2],
+                    help="neighbour-pass thread order: 0 hash, 1 Morton (default), 2 Morton cell-cooperative")
+    ap.add_argument("--sample", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
+                    help="smaller lattice of the same scene (profiling captures only)")
     return ap.parse_args()
 
 
@@ -224,9 +228,12 @@ def run_b200(args, dist):
     import pbf_b200 as P
     dev = dist.local
     torch.cuda.set_device(dev)
-    cfg, pos, vel, sdf, desc = workload(args.workload)
+    cfg, pos, vel, sdf, desc = workload(args.workload, sample=args.sample)
+    if args.sample:
+        desc = f"profiling sample {args.sample} of: " + desc
     n = len(pos)
     fl = P.PBFluids(cfg, device=dev)
+    fl.set_option(1, args.mode)
     fl.setParticles(P.make_particles(pos, vel))
     obstacle = None
     if sdf is not None:

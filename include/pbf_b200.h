@@ -268,6 +268,13 @@ int pbf_kernel_launches(pbf_handle* h, uint64_t* out);
 /* CUDA-graph replay of one full step (captured lazily, invalidated by any
  * parameter, particle or SDF change). */
 int pbf_set_use_graph(pbf_handle* h, int on);
+/* Execution options (results do not depend on them; no reference counterpart):
+ *   PBF_OPT_SPATIAL_ORDER  1 (default): neighbour passes take particles in the
+ *                          Morton order of their cells, one thread each;
+ *                          2: Morton order, one warp per cell with lanes
+ *                          sharing the candidate walk; 0: hash order. */
+#define PBF_OPT_SPATIAL_ORDER 1
+int pbf_set_option(pbf_handle* h, int option, int value);
 
 /* ---- health ------------------------------------------------------------- */
 /* Scan committed state for NaN/Inf; *bad receives the count (0 = healthy). */

@@ -180,7 +180,9 @@ __global__ void k_lbvh_refit(MeshDev M)
     M.bmax[node] = make_float4(fmaxf(A.x, fmaxf(B.x, C.x)), fmaxf(A.y, fmaxf(B.y, C.y)), fmaxf(A.z, fmaxf(B.z, C.z)), 0.f);
     __threadfence();
     int p = M.parent[node];
-    while (p >= 0) {
+    // a Karras tree over 30-bit codes with index tie-breaks is < 64 levels deep;
+    // the bound only guards against a malformed topology
+    for (int level = 0; p >= 0 && level < 128; ++level) {
         if (atomicAdd(&M.flags[p], 1u) == 0u) return;  // first arrival: the sibling finishes the parent
         const int2 ch = M.child[p];
         const float4 l0 = __ldcg(M.bmin + ch.x), l1 = __ldcg(M.bmax + ch.x);

