@@ -255,6 +255,23 @@ int pbf_sort_keys(const uint32_t* keys, uint32_t n, uint32_t key_bits,
 int pbf_build_table(const uint32_t* sorted_keys, uint32_t n, uint32_t hash_size,
                     int32_t* table);
 
+/* Allocation-free variant of the stable (key, id) radix sort, for callers that
+ * cannot call cudaMalloc (device memory owned by another framework's pool,
+ * plugins handed only device buffers, real-time loops that must not enter the
+ * allocator).  No counterpart in the reference.  keys_dev, sorted_keys_dev and
+ * sorted_ids_dev are caller-owned device arrays of n uint32 (keys must not
+ * alias the outputs); the work is queued on `stream` (a cudaStream_t, NULL for
+ * the default stream) and the call returns without synchronizing.  Scratch
+ * comes from one fixed device array of the library (about 8.3 MB, kept by
+ * every GPU that loads the library until exit), so n is limited to
+ * PBF_NOALLOC_MAX_KEYS, and calls whose GPU work overlaps (other streams or
+ * host threads) race on that array.  The first call on a device looks up the
+ * array's device address; make it before capturing that device's streams into
+ * a CUDA graph.  Keys wider than key_bits are ordered by their low key_bits. */
+#define PBF_NOALLOC_MAX_KEYS (1u << 20)
+int pbf_sort_keys_noalloc(const uint32_t* keys_dev, uint32_t n, uint32_t key_bits,
+                          uint32_t* sorted_keys_dev, uint32_t* sorted_ids_dev, void* stream);
+
 /* ---- timing ------------------------------------------------------------- */
 /* When on, every pass of pbf_step records CUDA events on the handle's stream
  * and accumulates per-pass device time (read with pbf_read_pass_times).

@@ -203,6 +203,21 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_downsweep(
     }
 }
 
+// Same sort, with the result guaranteed to land in (out_k, out_i): the first
+// pass writes to whichever pair makes the last pass end there, so the
+// caller's output arrays double as one half of the ping-pong and only one
+// more pair of scratch arrays is needed.
+void launch_radix_sort_into(uint32_t n, uint32_t key_bits, const uint32_t* keys_in, uint32_t* out_k, uint32_t* out_i,
+                            uint32_t* tmp_k, uint32_t* tmp_i, uint32_t* hist, uint32_t* totals, cudaStream_t st)
+{
+    if (key_bits == 0) key_bits = 1;
+    const uint32_t passes = (key_bits + 7u) / 8u;
+    const bool odd = (passes & 1u) != 0;
+    uint32_t *rk = nullptr, *ri = nullptr;
+    launch_radix_sort(n, key_bits, keys_in, odd ? out_k : tmp_k, odd ? out_i : tmp_i, odd ? tmp_k : out_k,
+                      odd ? tmp_i : out_i, hist, totals, &rk, &ri, st, nullptr);
+}
+
 // Sorts keys_in (particle order, left untouched) with ids 0..n-1, ping-ponging
 // between the (ka, ia) and (kb, ib) buffers; *out_keys / *out_ids receive the
 // pair holding the result.

@@ -54,6 +54,8 @@ uint32_t sort_num_tiles(uint32_t n);
 void launch_radix_sort(uint32_t n, uint32_t key_bits, const uint32_t* keys_in, uint32_t* ka, uint32_t* ia,
                        uint32_t* kb, uint32_t* ib, uint32_t* hist, uint32_t* totals, uint32_t** out_keys,
                        uint32_t** out_ids, cudaStream_t st, uint64_t* launches);
+void launch_radix_sort_into(uint32_t n, uint32_t key_bits, const uint32_t* keys_in, uint32_t* out_k, uint32_t* out_i,
+                            uint32_t* tmp_k, uint32_t* tmp_i, uint32_t* hist, uint32_t* totals, cudaStream_t st);
 
 // ---- k_sdf.cu -----------------------------------------------------------------
 void launch_sdf_slab_min(const float* dist, int dx, int dy, int dz, float* slab_min, cudaStream_t st);

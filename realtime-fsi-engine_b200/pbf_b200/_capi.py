@@ -125,6 +125,7 @@ SIGNATURES = [
     ("pbf_buffer_device_ptr", C.c_int, [vp, C.c_int, P(vp), P(C.c_size_t)]),
     ("pbf_sort_keys", C.c_int, [vp, u32, u32, vp, vp]),
     ("pbf_build_table", C.c_int, [vp, u32, u32, vp]),
+    ("pbf_sort_keys_noalloc", C.c_int, [vp, u32, u32, vp, vp, vp]),
     ("pbf_set_profiling", C.c_int, [vp, C.c_int]),
     ("pbf_read_pass_times", C.c_int, [vp, P(C.c_double), P(C.c_uint64)]),
     ("pbf_reset_pass_times", C.c_int, [vp]),
