@@ -286,10 +286,19 @@ int pbf_kernel_launches(pbf_handle* h, uint64_t* out);
  * parameter, particle or SDF change). */
 int pbf_set_use_graph(pbf_handle* h, int on);
 /* Execution options (results do not depend on them; no reference counterpart):
- *   PBF_OPT_SPATIAL_ORDER  1 (default): neighbour passes take particles in the
- *                          Morton order of their cells, one thread each;
- *                          2: Morton order, one warp per cell with lanes
- *                          sharing the candidate walk; 0: hash order. */
+ *   PBF_OPT_SPATIAL_ORDER  4 (default): neighbour passes take particles in the
+ *                          Morton order of their cells, one thread each, and
+ *                          test each bucket in chunks of 8 before running the
+ *                          pair body on the hits; 1: Morton order, body inside
+ *                          the candidate loop; 2: Morton order, one warp per
+ *                          cell with lanes sharing the candidate walk;
+ *                          3: Morton order, in-range pairs queued per lane and
+ *                          drained warp-wide; 5: Morton order, the distinct
+ *                          buckets of each 256-particle block staged once in
+ *                          shared memory (falls back to global reads when a
+ *                          block's buckets exceed the stage); 0: hash order.
+ *                          Every mode gives the same results up to FP32
+ *                          contraction differences. */
 #define PBF_OPT_SPATIAL_ORDER 1
 int pbf_set_option(pbf_handle* h, int option, int value);
 

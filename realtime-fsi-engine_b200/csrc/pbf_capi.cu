@@ -416,6 +416,12 @@ int pbf_handle::stage(int st, uint32_t iter)
         prof_begin(PBF_STAGE_LAMBDA);
         if (pass_mode == 2)
             launch_lambda_coop(P, sx[0], sx[1], rho, table, lod, iter, order, run_starts, scalars + 2, sms, stream);
+        else if (pass_mode == 3)
+            launch_lambda_q(P, sx[0], sx[1], rho, table, lod, iter, order, stream);
+        else if (pass_mode == 4)
+            launch_lambda_m(P, sx[0], sx[1], rho, table, lod, iter, order, stream);
+        else if (pass_mode == 5)
+            launch_lambda_s(P, sx[0], sx[1], rho, table, lod, iter, order, device, stream);
         else
             launch_lambda(P, sx[0], sx[1], rho, table, lod, iter, order, stream);
         ++launches;
@@ -426,6 +432,12 @@ int pbf_handle::stage(int st, uint32_t iter)
         prof_begin(PBF_STAGE_DELTAP);
         if (pass_mode == 2)
             launch_deltap_coop(P, sx[1], sx[0], table, lod, iter, order, run_starts, scalars + 2, sms, stream);
+        else if (pass_mode == 3)
+            launch_deltap_q(P, sx[1], sx[0], table, lod, iter, order, stream);
+        else if (pass_mode == 4)
+            launch_deltap_m(P, sx[1], sx[0], table, lod, iter, order, stream);
+        else if (pass_mode == 5)
+            launch_deltap_s(P, sx[1], sx[0], table, lod, iter, order, device, stream);
         else
             launch_deltap_apply(P, sx[1], sx[0], table, lod, iter, order, stream);
         ++launches;
@@ -437,6 +449,12 @@ int pbf_handle::stage(int st, uint32_t iter)
         if (pass_mode == 2)
             launch_integrate_coop(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, run_starts, scalars + 2,
                                   sms, stream);
+        else if (pass_mode == 3)
+            launch_integrate_q(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, stream);
+        else if (pass_mode == 4)
+            launch_integrate_m(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, stream);
+        else if (pass_mode == 5)
+            launch_integrate_s(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, device, stream);
         else
             launch_integrate(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, stream);
         ++launches;
@@ -446,6 +464,12 @@ int pbf_handle::stage(int st, uint32_t iter)
         prof_begin(PBF_STAGE_VORTICITY);
         if (pass_mode == 2)
             launch_vorticity_coop(P, sx0, somega, ids, vel, table, order, run_starts, scalars + 2, sms, stream);
+        else if (pass_mode == 3)
+            launch_vorticity_q(P, sx0, somega, ids, vel, table, order, stream);
+        else if (pass_mode == 4)
+            launch_vorticity_m(P, sx0, somega, ids, vel, table, order, stream);
+        else if (pass_mode == 5)
+            launch_vorticity_s(P, sx0, somega, ids, vel, table, order, device, stream);
         else
             launch_vorticity(P, sx0, somega, ids, vel, table, order, stream);
         ++launches;
@@ -532,6 +556,7 @@ extern "C" int pbf_create(const pbf_fluid_config* cfg, int device, pbf_handle** 
     h->cfg = *cfg;
     for (int i = 0; i < PBF_NUM_PASS_SLOTS; ++i) h->prof_open[i] = -1;
     cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
+    staged_init(device);
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         delete h;
@@ -1020,7 +1045,7 @@ extern "C" int pbf_set_option(pbf_handle* h, int option, int value)
     if (!h) return set_error(PBF_ERR_INVALID, "null handle");
     switch (option) {
     case PBF_OPT_SPATIAL_ORDER:
-        if (value < 0 || value > 2) return set_error(PBF_ERR_INVALID, "spatial order mode %d", value);
+        if (value < 0 || value > 5) return set_error(PBF_ERR_INVALID, "spatial order mode %d", value);
         h->pass_mode = value;
         break;
     default: return set_error(PBF_ERR_INVALID, "unknown option %d", option);

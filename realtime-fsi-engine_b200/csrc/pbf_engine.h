@@ -41,7 +41,9 @@ struct pbf_handle {
     int2* table = nullptr;
     // spatial processing order of the neighbour passes (Morton order of the
     // predict-time cells); `order` points into one of the m* ping-pong pairs
-    int pass_mode = 1;  // PBF_OPT_SPATIAL_ORDER: 0 hash order, 1 Morton order, 2 Morton cell-cooperative
+    // PBF_OPT_SPATIAL_ORDER: 0 hash order, 1 Morton order, 2 Morton cell-cooperative,
+    // 3 Morton + per-lane pair queues, 4 Morton + per-bucket hit masks (default)
+    int pass_mode = 4;
     uint32_t *mcode = nullptr, *mka = nullptr, *mia = nullptr, *mkb = nullptr, *mib = nullptr;
     uint32_t* order = nullptr;
     // cell runs of the Morton order (one warp per run in the cooperative passes)

@@ -49,6 +49,40 @@ void launch_vorticity_coop(const DevParams& P, const float4* spos, const float4*
                            float4* vel, const int2* table, const uint32_t* order, const uint32_t* runs,
                            const uint32_t* run_count, int sms, cudaStream_t st);
 
+// ---- k_queue.cu: thread per particle, in-range pairs queued per lane ---------
+void launch_lambda_q(const DevParams& P, const float4* xin, float4* xout, float* rho, const int2* table,
+                     const uint32_t* lod, uint32_t iter, const uint32_t* order, cudaStream_t st);
+void launch_deltap_q(const DevParams& P, const float4* xin, float4* xout, const int2* table, const uint32_t* lod,
+                     uint32_t iter, const uint32_t* order, cudaStream_t st);
+void launch_integrate_q(const DevParams& P, const float4* xs, const float4* sv, float4* sx0, float4* somega,
+                        const uint32_t* ids, float4* pos, float4* vel, const int2* table, const uint32_t* order,
+                        cudaStream_t st);
+void launch_vorticity_q(const DevParams& P, const float4* spos, const float4* somega, const uint32_t* ids,
+                        float4* vel, const int2* table, const uint32_t* order, cudaStream_t st);
+
+// ---- k_masked.cu: thread per particle, bucket chunks tested into a hit mask --
+void launch_lambda_m(const DevParams& P, const float4* xin, float4* xout, float* rho, const int2* table,
+                     const uint32_t* lod, uint32_t iter, const uint32_t* order, cudaStream_t st);
+void launch_deltap_m(const DevParams& P, const float4* xin, float4* xout, const int2* table, const uint32_t* lod,
+                     uint32_t iter, const uint32_t* order, cudaStream_t st);
+void launch_integrate_m(const DevParams& P, const float4* xs, const float4* sv, float4* sx0, float4* somega,
+                        const uint32_t* ids, float4* pos, float4* vel, const int2* table, const uint32_t* order,
+                        cudaStream_t st);
+void launch_vorticity_m(const DevParams& P, const float4* spos, const float4* somega, const uint32_t* ids,
+                        float4* vel, const int2* table, const uint32_t* order, cudaStream_t st);
+
+// ---- k_staged.cu: 256-particle cell blocks staged through shared memory -------
+void staged_init(int device);  // opt the kernels into > 48 KB of shared memory
+void launch_lambda_s(const DevParams& P, const float4* xin, float4* xout, float* rho, const int2* table,
+                     const uint32_t* lod, uint32_t iter, const uint32_t* order, int device, cudaStream_t st);
+void launch_deltap_s(const DevParams& P, const float4* xin, float4* xout, const int2* table, const uint32_t* lod,
+                     uint32_t iter, const uint32_t* order, int device, cudaStream_t st);
+void launch_integrate_s(const DevParams& P, const float4* xs, const float4* sv, float4* sx0, float4* somega,
+                        const uint32_t* ids, float4* pos, float4* vel, const int2* table, const uint32_t* order,
+                        int device, cudaStream_t st);
+void launch_vorticity_s(const DevParams& P, const float4* spos, const float4* somega, const uint32_t* ids,
+                        float4* vel, const int2* table, const uint32_t* order, int device, cudaStream_t st);
+
 // ---- k_sort.cu ----------------------------------------------------------------
 uint32_t sort_num_tiles(uint32_t n);
 void launch_radix_sort(uint32_t n, uint32_t key_bits, const uint32_t* keys_in, uint32_t* ka, uint32_t* ia,

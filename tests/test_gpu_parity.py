@@ -86,7 +86,9 @@ def test_cell_table_bit_exact(have_gpu):
 # ---- substep stages against the oracle (GPU inputs -> FP64) ---------------------------
 @pytest.mark.parametrize("name,mode", [(f, 1) for f in STAGE_FIXTURES] +
                          [("glsl_stages_scorr.npz", 2), ("glsl_stages_apbf.npz", 2), ("glsl_stages_sdf.npz", 2),
-                          ("glsl_stages_plain.npz", 0)])
+                          ("glsl_stages_plain.npz", 0)] +
+                         [(f, 3) for f in STAGE_FIXTURES] + [(f, 4) for f in STAGE_FIXTURES] +
+                         [(f, 5) for f in STAGE_FIXTURES])
 def test_stages_match_oracle(have_gpu, name, mode):
     z = H.load(name)
     fl, sdf = make_fluid(z, mode)
@@ -294,6 +296,28 @@ def test_contact_filter_deterministic_and_exact(have_gpu):
     assert len(fl.readbackContactCandidates()) == c
 
 
+def test_staged_blocks_fall_back_when_sparse(have_gpu):
+    """Scattered particles give a block more distinct buckets than its shared
+    hash set holds: the staged passes (mode 5) must read from global memory
+    and still match the per-thread masked passes (mode 4)."""
+    cfg, _, _ = scenes.c0(8)
+    rng = np.random.default_rng(8)
+    pos = rng.uniform(0.05, 0.95, size=(3000, 3)).astype(np.float32) * np.array([1.5, 0.9, 0.9], np.float32)
+    pos[:1000] = pos[:1000] * 0.1 + 0.3  # and a dense clump
+    vel = rng.uniform(-0.5, 0.5, size=pos.shape).astype(np.float32)
+    cfg.enable_scorr = 0
+    cfg.particle_count = len(pos)
+    outs = []
+    for mode in (4, 5):
+        fl = P.PBFluids(cfg)
+        fl.set_option(1, mode)
+        fl.setParticles(P.make_particles(pos, vel))
+        fl.step()
+        outs.append(fl.readbackParticles())
+    assert np.abs(outs[0]["pos"] - outs[1]["pos"]).max() < 1e-5 * cfg.h
+    assert np.abs(outs[0]["vel"] - outs[1]["vel"]).max() < 1e-3
+
+
 def test_cooperative_and_per_thread_passes_agree(have_gpu):
     """Thread order (hash / Morton) does not change a particle's arithmetic:
     bit-identical.  The cell-cooperative passes split each sum over lanes:
@@ -301,7 +325,7 @@ def test_cooperative_and_per_thread_passes_agree(have_gpu):
     cfg, pos, vel = scenes.c0(16, seed=4)
     cfg.enable_scorr = 0
     outs = {}
-    for mode in (1, 0, 2, 2):
+    for mode in (1, 0, 2, 2, 3, 3, 4, 5, 5):
         fl = P.PBFluids(cfg)
         fl.set_option(1, mode)
         fl.setParticles(P.make_particles(pos, vel))
@@ -311,5 +335,6 @@ def test_cooperative_and_per_thread_passes_agree(have_gpu):
             assert np.array_equal(outs[mode]["pos"], o["pos"]) and np.array_equal(outs[mode]["vel"], o["vel"])
         outs[mode] = o
     assert np.array_equal(outs[0]["pos"], outs[1]["pos"]) and np.array_equal(outs[0]["vel"], outs[1]["vel"])
-    assert np.abs(outs[2]["pos"] - outs[1]["pos"]).max() < 1e-5 * cfg.h
-    assert np.abs(outs[2]["vel"] - outs[1]["vel"]).max() < 1e-3
+    for m in (2, 3, 4, 5):
+        assert np.abs(outs[m]["pos"] - outs[1]["pos"]).max() < 1e-5 * cfg.h
+        assert np.abs(outs[m]["vel"] - outs[1]["vel"]).max() < 1e-3
