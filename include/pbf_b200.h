@@ -306,6 +306,83 @@ int pbf_set_option(pbf_handle* h, int option, int value);
 /* Scan committed state for NaN/Inf; *bad receives the count (0 = healthy). */
 int pbf_check_finite(pbf_handle* h, uint32_t* bad);
 
+/* ---- batched scenes ---------------------------------------------------------
+ * No reference counterpart: the reference steps one scene per PBFluids
+ * object (src/fluid/PBFluids.cpp:323-517).  A batch advances many independent
+ * scenes of uneven particle counts that share the solver constants of one
+ * pbf_fluid_config (h, dt, substeps, iterations, s_corr, XSPH, vorticity),
+ * each with its own walls, hash size and SDF obstacle, by one launch per
+ * pass over all scenes; the step is replayed from a CUDA graph.  Every scene
+ * evolves exactly as a pbf_handle with the same configuration would (same
+ * neighbour visitation, same per-pair arithmetic).  Not thread-safe per
+ * batch; distinct batches are independent. */
+typedef struct pbf_batch pbf_batch;
+
+typedef struct pbf_scene_desc {
+    uint32_t num_particles;
+    uint32_t hash_size;      /* power of two; 0 = the shared config's hash_size */
+    float bounds_min[3];     /* container walls, as FluidConfig::boundsMin/Max */
+    float bounds_max[3];
+} pbf_scene_desc;
+
+#define PBF_BATCH_ALL 0xFFFFFFFFu /* scene index meaning "all scenes, concatenated" */
+
+int pbf_batch_create(const pbf_fluid_config* cfg, const pbf_scene_desc* scenes, uint32_t num_scenes, int device,
+                     pbf_batch** out);
+int pbf_batch_destroy(pbf_batch* b);
+/* Scene count and total particle count. */
+int pbf_batch_info(const pbf_batch* b, uint32_t* num_scenes, uint32_t* total_particles);
+/* First particle index of `scene` in the concatenated arrays and its count. */
+int pbf_batch_scene_range(const pbf_batch* b, uint32_t scene, uint32_t* offset, uint32_t* count);
+/* Wall padding of every scene (PBFluids::setCollisionPadding). */
+int pbf_batch_set_collision_padding(pbf_batch* b, float padding);
+/* Particles of one scene (n = its count) or, with PBF_BATCH_ALL, of all
+ * scenes concatenated (n = total).  Velocities of the vorticity state are
+ * reset as pbf_set_particles does. */
+int pbf_batch_set_particles(pbf_batch* b, uint32_t scene, const pbf_particle* particles, uint32_t n);
+int pbf_batch_read_particles(pbf_batch* b, uint32_t scene, pbf_particle* out, uint32_t n);
+/* SDF obstacle of one scene: a distance grid in the layout of
+ * pbf_set_sdf_grid; pbf_batch_set_sdf_mode sets its padding/containment. */
+int pbf_batch_set_sdf_grid(pbf_batch* b, uint32_t scene, const float* dist, const int32_t dims[3],
+                           const float origin[3], float cell);
+int pbf_batch_set_sdf_mode(pbf_batch* b, uint32_t scene, float padding, uint32_t containment);
+int pbf_batch_clear_sdf(pbf_batch* b, uint32_t scene);
+/* One step() of every scene (substeps x iterations + vorticity), async. */
+int pbf_batch_step(pbf_batch* b);
+int pbf_batch_sync(pbf_batch* b);
+int pbf_batch_get_stream(pbf_batch* b, void** stream);
+/* Device arrays of the concatenated particles: float4 (x, pad0) and float4
+ * (v, pad2) in particle order; valid until pbf_batch_destroy. */
+int pbf_batch_device_ptrs(pbf_batch* b, void** pos4, void** vel4);
+int pbf_batch_kernel_launches(const pbf_batch* b, uint64_t* count);
+
+/* Options.  None changes results, only speed.
+ *   PBF_BOPT_BLOCK          threads per block of the neighbour passes: 64, 128 (default), 256
+ *   PBF_BOPT_ORDER          1 (default): threads take particles in the scene-prefixed
+ *                           Morton order of their cells; 0: sorted (hash) order
+ *   PBF_BOPT_BLOCKS_PER_SM  persistent grid of SMs x value blocks looping over the
+ *                           particles; 0 (default): one thread per particle
+ *   PBF_BOPT_USE_GRAPH      1 (default): replay the step from a CUDA graph */
+#define PBF_BOPT_BLOCK 1
+#define PBF_BOPT_ORDER 2
+#define PBF_BOPT_BLOCKS_PER_SM 3
+#define PBF_BOPT_USE_GRAPH 4
+int pbf_batch_set_option(pbf_batch* b, int option, int value);
+int pbf_batch_get_option(const pbf_batch* b, int option, int* value);
+
+typedef struct pbf_batch_tuning {
+    int32_t block;
+    int32_t order;
+    int32_t blocks_per_sm;
+    float ms_per_step;
+} pbf_batch_tuning;
+/* Times every candidate (block x order x persistence) for `trial_steps` steps
+ * after one warm-up step, keeps the fastest and restores the particle state
+ * that the trials advanced.  `results` (may be null) receives up to
+ * `max_results` timed candidates, `*num_results` their count; `*best` the pick. */
+int pbf_batch_autotune(pbf_batch* b, uint32_t trial_steps, pbf_batch_tuning* best, pbf_batch_tuning* results,
+                       uint32_t max_results, uint32_t* num_results);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -1,0 +1,274 @@
+// masked_body.cuh — per-particle bodies of the neighbour passes, shared by
+// the single-scene kernels (k_masked.cu) and the multi-scene kernels
+// (k_batch.cu) so that both run the same arithmetic on every pair.
+//
+// Each function takes the scene's bucket table (already offset to the
+// scene's first bucket), its hash mask and, where the pass needs them, the
+// scene's walls and SDF; everything else comes from DevParams.
+//
+// Walk: for each of the particle's 27 buckets (CS_ComputeLambdas.glsl:126-150,
+// z outer, x inner), up to 8 candidates are loaded with independent
+// predicated loads and reduced to an 8-bit mask of in-range pairs; the body
+// then runs for the set bits in candidate order.  The candidate multiset,
+// its per-bucket order and each pair's arithmetic match the sequential loop
+// of the reference, so sums are accumulated in the same order as there.
+#pragma once
+
+#include "pbf_internal.cuh"
+
+namespace pbf {
+
+constexpr int kChunk = 8;
+
+template <class Hit, class Body>
+__device__ __forceinline__ void masked_walk(const DevParams& P, const int2* __restrict__ table, uint32_t mask,
+                                            const float4* __restrict__ X, float xi, float yi, float zi, int self,
+                                            Hit&& hit, Body&& body)
+{
+    const int cx = cell_coord(xi, P.h), cy = cell_coord(yi, P.h), cz = cell_coord(zi, P.h);
+#pragma unroll 1
+    for (int dz = -1; dz <= 1; ++dz) {
+        const uint32_t hz = (uint32_t)(cz + dz) * kP3;
+#pragma unroll 1
+        for (int dy = -1; dy <= 1; ++dy) {
+            const uint32_t hyz = hz ^ ((uint32_t)(cy + dy) * kP2);
+#pragma unroll 1
+            for (int dx = -1; dx <= 1; ++dx) {
+                const uint32_t hsh = (((uint32_t)(cx + dx) * kP1) ^ hyz) & mask;
+                const int2 se = __ldg(table + hsh);
+                if (se.x == -1) continue;
+#pragma unroll 1
+                for (int k0 = se.x; k0 < se.y; k0 += kChunk) {
+                    uint32_t m = 0;
+#pragma unroll
+                    for (int c = 0; c < kChunk; ++c) {
+                        const int k = k0 + c;
+                        if (k < se.y) {
+                            const float4 xj = __ldg(X + k);
+                            const float rx = xi - xj.x, ry = yi - xj.y, rz = zi - xj.z;
+                            const float r2 = rx * rx + ry * ry + rz * rz;
+                            if (hit(r2) && k != self) m |= 1u << c;
+                        }
+                    }
+                    while (m) {
+                        const int c = __ffs(m) - 1;
+                        m &= m - 1u;
+                        body(k0 + c);
+                    }
+                }
+            }
+        }
+    }
+}
+
+// ---- CS_ComputeLambdas.glsl:108-162: returns (x*, lambda), writes rho ----------------------
+__device__ __forceinline__ float4 lambda_particle(const DevParams& P, const int2* __restrict__ table, uint32_t mask,
+                                                  const float4* __restrict__ xin, int s, float& rho_out)
+{
+    const float4 xi = __ldg(xin + s);
+    float rho = P.w0_self, sg = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+    masked_walk(
+        P, table, mask, xin, xi.x, xi.y, xi.z, s, [&](float r2) { return r2 <= P.h2; },
+        [&](int k) {
+            const float4 xj = __ldg(xin + k);
+            const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+            const float r2 = rx * rx + ry * ry + rz * rz;
+            rho += poly6_in(P, r2);
+            if (r2 >= 1e-10f) {
+                const float sc = spiky_scale(P, r2);
+                const float ax = rx * sc, ay = ry * sc, az = rz * sc;
+                sg += (ax * ax + ay * ay + az * az) * P.inv_rho0_sq;
+                gx += ax;
+                gy += ay;
+                gz += az;
+            }
+        });
+    gx *= P.inv_rho0;
+    gy *= P.inv_rho0;
+    gz *= P.inv_rho0;
+    const float C = fmaxf(rho / P.rho0 - 1.0f, -P.cohesion);
+    sg += gx * gx + gy * gy + gz * gz;
+    rho_out = rho;
+    return make_float4(xi.x, xi.y, xi.z, -C / (sg + P.eps));
+}
+
+// s_corr * (poly6 coefficient form) of CS_ComputeDeltaP.glsl:94-104 added to
+// lambda_i + lambda_j; valid for r2 < h2.
+__device__ __forceinline__ float scorr_term(const DevParams& P, float r2)
+{
+    const float d = P.h2 - r2;
+    const float w = P.poly6 * d * d * d;
+    if (P.wq > 1e-12f && w > 0.0f) {
+        const float ratio = w * P.inv_wq;
+        float pw;
+        if (P.ncorr_is4) {
+            const float q = ratio * ratio;
+            pw = q * q;
+        } else {
+            pw = powf(ratio, P.n_corr);
+        }
+        return -P.k_corr * pw;
+    }
+    return 0.0f;
+}
+
+// ---- CS_ComputeDeltaP.glsl:120-166 + CS_ApplyDeltaP.glsl:80-124: returns (x* + dp, lambda) -----
+__device__ __forceinline__ float4 deltap_particle(const DevParams& P, const int2* __restrict__ table, uint32_t mask,
+                                                  const SdfDev& sdf, const float4* __restrict__ xin, int s)
+{
+    const float4 xi = __ldg(xin + s);
+    const float li = xi.w;
+    float dx = 0.f, dy = 0.f, dz = 0.f;
+    masked_walk(
+        P, table, mask, xin, xi.x, xi.y, xi.z, s, [&](float r2) { return r2 <= P.h2 && r2 >= 1e-10f; },
+        [&](int k) {
+            const float4 xj = __ldg(xin + k);
+            const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+            const float r2 = rx * rx + ry * ry + rz * rz;
+            const float sc = spiky_scale(P, r2);
+            float f = li + xj.w;
+            if (P.scorr) f += scorr_term(P, r2);
+            const float g = sc * f;
+            dx += rx * g;
+            dy += ry * g;
+            dz += rz * g;
+        });
+    dx *= P.inv_rho0;
+    dy *= P.inv_rho0;
+    dz *= P.inv_rho0;
+    const float l2 = dx * dx + dy * dy + dz * dz;
+    if (l2 > P.max_dp * P.max_dp) {
+        const float sc = P.max_dp * rsqrtf(l2);
+        dx *= sc;
+        dy *= sc;
+        dz *= sc;
+    }
+    float3 p = make_float3(xi.x + dx, xi.y + dy, xi.z + dz);
+    if (sdf.enabled) {
+        float3 nrm;
+        sdf_project(sdf, p, nrm);
+    }
+    return make_float4(p.x, p.y, p.z, li);
+}
+
+// ---- CS_Integrate.glsl:135-280 (pre-dispatch neighbour velocities) ---------------------------
+// Commits x and v of slot s: writes pos/vel at the particle id, sx0[s] = x
+// and somega[s] = (omega, |omega|).
+__device__ __forceinline__ void integrate_particle(const DevParams& P, const int2* __restrict__ table, uint32_t mask,
+                                                   const float* bmin, const float* bmax, const SdfDev& sdf,
+                                                   const float4* __restrict__ xs, const float4* __restrict__ sv,
+                                                   float4* __restrict__ sx0, float4* __restrict__ somega,
+                                                   const uint32_t* __restrict__ ids, float4* __restrict__ pos,
+                                                   float4* __restrict__ vel, int s)
+{
+    const float4 x4 = __ldg(xs + s);
+    const float4 v0 = __ldg(sv + s);
+    float fx = 0.f, fy = 0.f, fz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+    if (P.visc_on || P.vort_on) {
+        masked_walk(
+            P, table, mask, xs, x4.x, x4.y, x4.z, s, [&](float r2) { return r2 <= P.h2; },
+            [&](int k) {
+                const float4 xj = __ldg(xs + k);
+                const float rx = x4.x - xj.x, ry = x4.y - xj.y, rz = x4.z - xj.z;
+                const float r2 = rx * rx + ry * ry + rz * rz;
+                const float4 vj = __ldg(sv + k);
+                const float ux = vj.x - v0.x, uy = vj.y - v0.y, uz = vj.z - v0.z;
+                if (P.visc_on) {
+                    const float w = poly6_in(P, r2) * P.inv_rho0;
+                    fx += ux * w;
+                    fy += uy * w;
+                    fz += uz * w;
+                }
+                if (P.vort_on && r2 >= 1e-10f) {
+                    const float sc = spiky_scale(P, r2);
+                    const float ax = rx * sc, ay = ry * sc, az = rz * sc;
+                    cx += uy * az - uz * ay;
+                    cy += uz * ax - ux * az;
+                    cz += ux * ay - uy * ax;
+                }
+            });
+    }
+    const float4 p0 = sx0[s];
+    float3 x = make_float3(x4.x, x4.y, x4.z);
+    float vdx = 0.f, vdy = 0.f, vdz = 0.f;
+    if (P.visc_on) {
+        vdx = fx * P.viscosity;
+        vdy = fy * P.viscosity;
+        vdz = fz * P.viscosity;
+    }
+    if (P.vort_on) {
+        const float ox = cx * P.inv_rho0, oy = cy * P.inv_rho0, oz = cz * P.inv_rho0;
+        somega[s] = make_float4(ox, oy, oz, sqrtf(ox * ox + oy * oy + oz * oz));
+    }
+    bool colx = false, coly = false, colz = false;
+    if (x.x <= bmin[0]) { x.x = bmin[0]; colx = true; }
+    if (x.x >= bmax[0]) { x.x = bmax[0]; colx = true; }
+    if (x.y <= bmin[1]) { x.y = bmin[1]; coly = true; }
+    if (x.y >= bmax[1]) { x.y = bmax[1]; coly = true; }
+    if (x.z <= bmin[2]) { x.z = bmin[2]; colz = true; }
+    if (x.z >= bmax[2]) { x.z = bmax[2]; colz = true; }
+    bool col_sdf = false;
+    float3 nrm = make_float3(0.0f, 0.0f, 0.0f);
+    if (sdf.enabled) col_sdf = sdf_project(sdf, x, nrm);
+    float vx = (x.x - p0.x) * P.inv_dt + vdx;
+    float vy = (x.y - p0.y) * P.inv_dt + vdy;
+    float vz = (x.z - p0.z) * P.inv_dt + vdz;
+    const float sp2 = vx * vx + vy * vy + vz * vz;
+    if (sp2 > 2500.0f) {
+        const float sc = 50.0f / sqrtf(sp2);
+        vx *= sc;
+        vy *= sc;
+        vz *= sc;
+    }
+    if (colx) vx *= -P.damping;
+    if (coly) vy *= -P.damping;
+    if (colz) vz *= -P.damping;
+    if (col_sdf) {
+        const float vn = vx * nrm.x + vy * nrm.y + vz * nrm.z;
+        vx -= vn * nrm.x;
+        vy -= vn * nrm.y;
+        vz -= vn * nrm.z;
+    }
+    const uint32_t id = __ldg(ids + s);
+    const float4 xo = make_float4(x.x, x.y, x.z, p0.w);
+    pos[id] = xo;
+    vel[id] = make_float4(vx, vy, vz, v0.w);
+    sx0[s] = xo;
+}
+
+// ---- CS_VorticityConfinement.glsl:133-167 (pass 1) ----------------------------------------------
+__device__ __forceinline__ void vorticity_particle(const DevParams& P, const int2* __restrict__ table, uint32_t mask,
+                                                   const float4* __restrict__ spos,
+                                                   const float4* __restrict__ somega,
+                                                   const uint32_t* __restrict__ ids, float4* __restrict__ vel, int s)
+{
+    const float4 xi = __ldg(spos + s);
+    float ex = 0.f, ey = 0.f, ez = 0.f;
+    masked_walk(
+        P, table, mask, spos, xi.x, xi.y, xi.z, s, [&](float r2) { return r2 <= P.h2 && r2 >= 1e-10f; },
+        [&](int k) {
+            const float4 xj = __ldg(spos + k);
+            const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+            const float r2 = rx * rx + ry * ry + rz * rz;
+            const float sc = spiky_scale(P, r2) * __ldg(&somega[k].w);
+            ex += rx * sc;
+            ey += ry * sc;
+            ez += rz * sc;
+        });
+    ex *= P.inv_rho0;
+    ey *= P.inv_rho0;
+    ez *= P.inv_rho0;
+    const float el = sqrtf(ex * ex + ey * ey + ez * ez);
+    if (el < 1e-6f) return;
+    const float nx = ex / el, ny = ey / el, nz = ez / el;
+    const float4 w = __ldg(somega + s);
+    const float crx = ny * w.z - nz * w.y, cry = nz * w.x - nx * w.z, crz = nx * w.y - ny * w.x;
+    const uint32_t id = __ldg(ids + s);
+    float4 v = vel[id];
+    v.x += P.vort_eps * crx * P.dt;
+    v.y += P.vort_eps * cry * P.dt;
+    v.z += P.vort_eps * crz * P.dt;
+    vel[id] = v;
+}
+
+}  // namespace pbf

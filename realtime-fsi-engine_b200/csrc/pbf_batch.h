@@ -1,0 +1,114 @@
+// pbf_batch.h — the multi-scene engine behind the pbf_batch_* C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "../../include/pbf_b200.h"
+#include "pbf_kernels.h"
+
+namespace pbf {
+
+// Per-scene constants read by the multi-scene passes (device array, one
+// entry per scene).
+struct SceneDev {
+    uint32_t table_off;  // first bucket of the scene in the shared cell table
+    uint32_t mask;       // H_k - 1
+    float bmin[3], bmax[3];  // walls after collision padding (PBFluids::setBounds)
+    int cell_lo[3];      // lowest cell of the walls: origin of the Morton code
+    int pad_;
+    SdfDev sdf;
+};
+
+struct BatchLaunch {
+    int block = 128;         // threads per block of the neighbour passes
+    int blocks_per_sm = 0;   // persistent grid (0: one thread per particle)
+    int sms = 148;
+};
+
+void launch_b_predict(const DevParams& P, const SceneDev* scenes, const uint16_t* scene_of, const float4* pos,
+                      const float4* vel, uint32_t* keys, int sms, cudaStream_t st);
+void launch_b_reorder(const DevParams& P, const SceneDev* scenes, const uint16_t* scene_of, const uint32_t* ids,
+                      const float4* pos, const float4* vel, float4* sx, float4* sv, float4* sx0, uint32_t* lod,
+                      uint32_t* mcode, uint32_t mbits, int sms, cudaStream_t st);
+void launch_b_lambda(const DevParams& P, const BatchLaunch& L, const SceneDev* scenes, const uint16_t* scene_of,
+                     const float4* xin, float4* xout, float* rho, const int2* table, const uint32_t* lod,
+                     uint32_t iter, const uint32_t* order, cudaStream_t st);
+void launch_b_deltap(const DevParams& P, const BatchLaunch& L, const SceneDev* scenes, const uint16_t* scene_of,
+                     const float4* xin, float4* xout, const int2* table, const uint32_t* lod, uint32_t iter,
+                     const uint32_t* order, cudaStream_t st);
+void launch_b_integrate(const DevParams& P, const BatchLaunch& L, const SceneDev* scenes, const uint16_t* scene_of,
+                        const float4* xs, const float4* sv, float4* sx0, float4* somega, const uint32_t* ids,
+                        float4* pos, float4* vel, const int2* table, const uint32_t* order, cudaStream_t st);
+void launch_b_vorticity(const DevParams& P, const BatchLaunch& L, const SceneDev* scenes, const uint16_t* scene_of,
+                        const float4* spos, const float4* somega, const uint32_t* ids, float4* vel, const int2* table,
+                        const uint32_t* order, cudaStream_t st);
+int batch_max_blocks_per_sm(int block);
+
+}  // namespace pbf
+
+struct pbf_batch {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+
+    pbf_fluid_config cfg{};        // shared solver constants
+    pbf_derived_params derived{};  // of cfg (walls per scene)
+    float collision_padding = 0.0f;
+
+    struct Scene {
+        pbf_scene_desc desc{};
+        uint32_t offset = 0, table_off = 0;
+        float* grid = nullptr;
+        float* slab_min = nullptr;
+        int dims[3] = {0, 0, 0};
+        float origin[3] = {0, 0, 0};
+        float cell = 0.0f;
+        bool sdf_on = false;
+        float sdf_padding = 0.0f;
+        bool containment = false;
+    };
+    std::vector<Scene> scenes;
+    uint32_t n = 0;            // total particles
+    uint32_t table_size = 0;   // sum of H_k
+    uint32_t key_bits = 1;     // bits of the offset hash keys
+    uint32_t mbits = 8;        // Morton bits per axis
+    uint32_t order_bits = 24;  // bits of the scene-prefixed Morton keys
+
+    // particle order
+    float4 *pos = nullptr, *vel = nullptr, *pred = nullptr, *aos = nullptr;
+    uint16_t* scene_of = nullptr;
+    pbf::SceneDev* scenes_dev = nullptr;
+    uint32_t* keys = nullptr;
+    uint32_t *ka = nullptr, *ia = nullptr, *kb = nullptr, *ib = nullptr;
+    uint32_t *skeys = nullptr, *ids = nullptr;
+    uint32_t *hist = nullptr, *totals = nullptr;
+    int2* table = nullptr;
+    uint32_t *mcode = nullptr, *mka = nullptr, *mia = nullptr, *mkb = nullptr, *mib = nullptr;
+    uint32_t* order = nullptr;
+    // sorted order
+    float4 *sx[2] = {nullptr, nullptr}, *sv = nullptr, *sx0 = nullptr, *somega = nullptr;
+    float* rho = nullptr;
+    uint32_t* lod = nullptr;
+    // autotuner state snapshot
+    float4 *save_pos = nullptr, *save_vel = nullptr;
+
+    // options (PBF_BOPT_*)
+    pbf::BatchLaunch launch{};
+    int morton = 1;
+    bool use_graph = true;
+
+    uint64_t launches = 0;
+    bool capturing = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    uint64_t graph_launches = 0;
+
+    ~pbf_batch();
+    pbf::DevParams dev_params() const;
+    int upload_scenes();
+    void invalidate_graph();
+    int step_body();
+    int step();
+};

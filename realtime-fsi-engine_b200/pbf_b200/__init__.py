@@ -14,7 +14,8 @@ import numpy as np
 from ._capi import (BUF_KEYS, BUF_LOD, BUF_OMEGA, BUF_POS, BUF_RHO, BUF_SORTED_IDS, BUF_SORTED_KEYS, BUF_TABLE,
                     BUF_VEL, BUF_VPRED, BUF_XSTAR, NUM_PASS_SLOTS, PASS_NAMES, STAGE_DELTAP, STAGE_INTEGRATE,
                     STAGE_LAMBDA, STAGE_PREDICT, STAGE_REORDER, STAGE_SORT, STAGE_TABLE, STAGE_VORTICITY,
-                    ContactCandidate, DerivedParams, FluidConfig, Particle, PBFError, check, fvec, lib)
+                    BATCH_ALL, BOPT_BLOCK, BOPT_BLOCKS_PER_SM, BOPT_ORDER, BOPT_USE_GRAPH, BatchTuning,
+                    ContactCandidate, DerivedParams, FluidConfig, Particle, PBFError, SceneDesc, check, fvec, lib)
 
 # numpy view of Particle (48 bytes: pos, pad0, predPos, pad1, vel, pad2)
 PARTICLE_DTYPE = np.dtype([("pos", "<f4", 3), ("pad0", "<f4"), ("pred_pos", "<f4", 3), ("pad1", "<f4"),
@@ -365,6 +366,124 @@ class PBFluids:
         return s.value
 
 
+class Batch:
+    """Many independent scenes advanced by one launch per pass (pbf_batch_*).
+
+    ``scenes`` is a list of dicts with ``n`` (particle count), ``bounds_min``,
+    ``bounds_max`` and optionally ``hash_size``; the solver constants come
+    from ``cfg`` and are shared.  Every scene evolves as a ``PBFluids`` with
+    the same configuration would."""
+
+    def __init__(self, cfg, scenes, device=0):
+        self._b = C.c_void_p()
+        self._cfg = cfg
+        descs = (SceneDesc * len(scenes))()
+        for k, s in enumerate(scenes):
+            descs[k].num_particles = int(s["n"])
+            descs[k].hash_size = int(s.get("hash_size", 0))
+            descs[k].bounds_min[:] = [float(v) for v in s["bounds_min"]]
+            descs[k].bounds_max[:] = [float(v) for v in s["bounds_max"]]
+        check(lib().pbf_batch_create(C.byref(cfg), C.cast(descs, C.c_void_p), len(scenes), int(device),
+                                     C.byref(self._b)))
+        self.num_scenes, self.total = self.info()
+
+    def __del__(self):
+        self.close()
+
+    def close(self):
+        try:
+            if self._b:
+                lib().pbf_batch_destroy(self._b)
+                self._b = C.c_void_p()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._b
+
+    def info(self):
+        ns, nt = C.c_uint32(), C.c_uint32()
+        check(lib().pbf_batch_info(self._b, C.byref(ns), C.byref(nt)))
+        return ns.value, nt.value
+
+    def scene_range(self, k):
+        off, cnt = C.c_uint32(), C.c_uint32()
+        check(lib().pbf_batch_scene_range(self._b, int(k), C.byref(off), C.byref(cnt)))
+        return off.value, cnt.value
+
+    def _count(self, k):
+        return self.total if k == BATCH_ALL else self.scene_range(k)[1]
+
+    def set_collision_padding(self, pad):
+        check(lib().pbf_batch_set_collision_padding(self._b, float(pad)))
+
+    def set_particles(self, k, particles):
+        ps = np.ascontiguousarray(particles, dtype=PARTICLE_DTYPE)
+        check(lib().pbf_batch_set_particles(self._b, int(k), _ptr(ps) if len(ps) else None, len(ps)))
+
+    def read_particles(self, k=BATCH_ALL, out=None):
+        n = self._count(k)
+        if out is None:
+            out = np.zeros(n, PARTICLE_DTYPE)
+        check(lib().pbf_batch_read_particles(self._b, int(k), _ptr(out) if n else None, len(out)))
+        return out
+
+    def set_sdf_grid(self, k, dist, origin, cell):
+        g = np.ascontiguousarray(dist, dtype=np.float32)
+        dims = (C.c_int32 * 3)(*g.shape)
+        check(lib().pbf_batch_set_sdf_grid(self._b, int(k), _ptr(g), dims, fvec(origin), float(cell)))
+
+    def set_sdf_mode(self, k, padding, containment=False):
+        check(lib().pbf_batch_set_sdf_mode(self._b, int(k), float(padding), 1 if containment else 0))
+
+    def clear_sdf(self, k):
+        check(lib().pbf_batch_clear_sdf(self._b, int(k)))
+
+    def step(self):
+        check(lib().pbf_batch_step(self._b))
+
+    def sync(self):
+        check(lib().pbf_batch_sync(self._b))
+
+    def stream(self):
+        s = C.c_void_p()
+        check(lib().pbf_batch_get_stream(self._b, C.byref(s)))
+        return s.value
+
+    def device_ptrs(self):
+        p, v = C.c_void_p(), C.c_void_p()
+        check(lib().pbf_batch_device_ptrs(self._b, C.byref(p), C.byref(v)))
+        return p.value, v.value
+
+    def kernel_launches(self):
+        c = C.c_uint64()
+        check(lib().pbf_batch_kernel_launches(self._b, C.byref(c)))
+        return c.value
+
+    def set_option(self, option, value):
+        check(lib().pbf_batch_set_option(self._b, int(option), int(value)))
+
+    def get_option(self, option):
+        v = C.c_int()
+        check(lib().pbf_batch_get_option(self._b, int(option), C.byref(v)))
+        return v.value
+
+    def autotune(self, trial_steps=3):
+        """Pick block size, cell order and persistence by timing; returns
+        (best, [all candidates]) as dicts.  The particle state is restored."""
+        best = BatchTuning()
+        res = (BatchTuning * 32)()
+        cnt = C.c_uint32()
+        check(lib().pbf_batch_autotune(self._b, int(trial_steps), C.byref(best), C.cast(res, C.c_void_p), 32,
+                                       C.byref(cnt)))
+
+        def d(t):
+            return dict(block=t.block, order=t.order, blocks_per_sm=t.blocks_per_sm, ms_per_step=t.ms_per_step)
+
+        return d(best), [d(res[i]) for i in range(cnt.value)]
+
+
 def sort_keys(keys, key_bits):
     """Stable (key, id) radix sort on the GPU (the CS_Radix* contract)."""
     k = np.ascontiguousarray(keys, dtype=np.uint32)
@@ -385,7 +504,8 @@ def build_table(sorted_keys, hash_size):
 __all__ = [
     "PBFluids", "SDFBoundary", "GridSDF", "FluidConfig", "DerivedParams", "Particle", "ContactCandidate",
     "PARTICLE_DTYPE", "CONTACT_DTYPE", "default_config", "derive_params", "make_particles", "sort_keys",
-    "build_table", "PBFError", "lib",
+    "build_table", "PBFError", "lib", "Batch", "SceneDesc", "BATCH_ALL", "BOPT_BLOCK", "BOPT_ORDER",
+    "BOPT_BLOCKS_PER_SM", "BOPT_USE_GRAPH",
     "STAGE_PREDICT", "STAGE_SORT", "STAGE_TABLE", "STAGE_REORDER", "STAGE_LAMBDA", "STAGE_DELTAP",
     "STAGE_INTEGRATE", "STAGE_VORTICITY", "BUF_KEYS", "BUF_SORTED_KEYS", "BUF_SORTED_IDS", "BUF_TABLE",
     "BUF_XSTAR", "BUF_VPRED", "BUF_RHO", "BUF_OMEGA", "BUF_POS", "BUF_VEL", "BUF_LOD",

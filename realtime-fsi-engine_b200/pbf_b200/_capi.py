@@ -75,8 +75,26 @@ class ContactCandidate(C.Structure):
     _fields_ = [("pos", C.c_float * 4), ("vel", C.c_float * 4)]
 
 
+class SceneDesc(C.Structure):
+    """pbf_scene_desc: one scene of a batch (particle count, hash size, walls)."""
+
+    _fields_ = [("num_particles", C.c_uint32), ("hash_size", C.c_uint32), ("bounds_min", C.c_float * 3),
+                ("bounds_max", C.c_float * 3)]
+
+
+class BatchTuning(C.Structure):
+    """pbf_batch_tuning: one autotuner candidate and its time per step."""
+
+    _fields_ = [("block", C.c_int32), ("order", C.c_int32), ("blocks_per_sm", C.c_int32),
+                ("ms_per_step", C.c_float)]
+
+
+BATCH_ALL = 0xFFFFFFFF
+BOPT_BLOCK, BOPT_ORDER, BOPT_BLOCKS_PER_SM, BOPT_USE_GRAPH = 1, 2, 3, 4
+
 assert C.sizeof(Particle) == 48 and C.sizeof(ContactCandidate) == 32
 assert C.sizeof(DerivedParams) == 144
+assert C.sizeof(SceneDesc) == 32 and C.sizeof(BatchTuning) == 16
 
 vp = C.c_void_p
 i32 = C.c_int32
@@ -133,6 +151,25 @@ SIGNATURES = [
     ("pbf_set_use_graph", C.c_int, [vp, C.c_int]),
     ("pbf_set_option", C.c_int, [vp, C.c_int, C.c_int]),
     ("pbf_check_finite", C.c_int, [vp, P(u32)]),
+    # batched scenes
+    ("pbf_batch_create", C.c_int, [P(FluidConfig), vp, u32, C.c_int, P(vp)]),
+    ("pbf_batch_destroy", C.c_int, [vp]),
+    ("pbf_batch_info", C.c_int, [vp, P(u32), P(u32)]),
+    ("pbf_batch_scene_range", C.c_int, [vp, u32, P(u32), P(u32)]),
+    ("pbf_batch_set_collision_padding", C.c_int, [vp, C.c_float]),
+    ("pbf_batch_set_particles", C.c_int, [vp, u32, vp, u32]),
+    ("pbf_batch_read_particles", C.c_int, [vp, u32, vp, u32]),
+    ("pbf_batch_set_sdf_grid", C.c_int, [vp, u32, vp, P(i32), P(C.c_float), C.c_float]),
+    ("pbf_batch_set_sdf_mode", C.c_int, [vp, u32, C.c_float, u32]),
+    ("pbf_batch_clear_sdf", C.c_int, [vp, u32]),
+    ("pbf_batch_step", C.c_int, [vp]),
+    ("pbf_batch_sync", C.c_int, [vp]),
+    ("pbf_batch_get_stream", C.c_int, [vp, P(vp)]),
+    ("pbf_batch_device_ptrs", C.c_int, [vp, P(vp), P(vp)]),
+    ("pbf_batch_kernel_launches", C.c_int, [vp, P(C.c_uint64)]),
+    ("pbf_batch_set_option", C.c_int, [vp, C.c_int, C.c_int]),
+    ("pbf_batch_get_option", C.c_int, [vp, C.c_int, P(C.c_int)]),
+    ("pbf_batch_autotune", C.c_int, [vp, u32, vp, vp, u32, P(u32)]),
 ]
 
 _lib = None

@@ -176,9 +176,66 @@ def c2(seed=0, nx=256, ny=128, nz=128):
     return cfg, pos, np.zeros_like(pos), (grid, origin, cell, d / 2.0)
 
 
+def sphere_grid(radius, center, cell):
+    """Analytic sphere SDF on the reference grid layout (as capsule_grid)."""
+    c = np.asarray(center, np.float64)
+    buf = 5.0 * cell
+    origin = c - radius - buf
+    dims = np.full(3, int(np.ceil((2.0 * (radius + buf)) / cell)))
+    xs = [origin[k] + np.arange(dims[k]) * cell for k in range(3)]
+    X, Y, Z = np.meshgrid(*xs, indexing="ij")
+    dist = np.sqrt((X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2) - radius
+    return dist.astype(np.float32), origin, cell
+
+
+def block(n, d, box, jitter, seed):
+    """n particles in a cubic-ish lattice block at the box corner: side
+    ceil(cbrt n) cells in x and z (capped to the box), rows stacked in y, the
+    top layer partial (x fastest, then z, then y)."""
+    side = int(math.ceil(round(n ** (1.0 / 3.0), 9)))
+    nx = max(1, min(side, int(box[0] / d) - 1))
+    nz = max(1, min(side, int(box[2] / d) - 1))
+    ny = int(math.ceil(n / (nx * nz)))
+    if ny * d > box[1]:  # too tall for the box: spread over the whole floor
+        nx = max(1, int(box[0] / d) - 1)
+        nz = max(1, int(box[2] / d) - 1)
+        ny = int(math.ceil(n / (nx * nz)))
+    j, k, i = np.meshgrid(np.arange(ny), np.arange(nz), np.arange(nx), indexing="ij")
+    g = np.stack([i.ravel(), j.ravel(), k.ravel()], axis=1)[:n].astype(np.float64)
+    pos = (g + 0.5) * d
+    if jitter > 0:
+        pos += np.random.default_rng(seed).uniform(-jitter, jitter, size=pos.shape)
+    return pos.astype(np.float32)
+
+
 def c3_sizes(seed=7, count=64):
     rng = np.random.default_rng(seed)
     return rng.integers(4096, 131072 + 1, size=count)
+
+
+def c3(seed=7, count=64, sizes=None):
+    """C3: `count` independent dam breaks sharing the C0 constants (d=0.02,
+    h=0.04, S=2, I=4, H=2^17 per scene).  From one generator seeded `seed`:
+    N_i ~ U[4096, 131072], box per axis ~ U[0.8, 1.6], sphere radius ~
+    U[0.05, 0.2]; the sphere sits at (0.75 bx, 0.3 by, 0.5 bz), padding d/2.
+    Returns (cfg, scenes), each scene a dict with n, bounds_min, bounds_max,
+    pos, vel and sdf = (grid, origin, cell, padding)."""
+    d, h = 0.02, 0.04
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(4096, 131072 + 1, size=count) if sizes is None else np.asarray(sizes)
+    boxes = rng.uniform(0.8, 1.6, size=(count, 3))
+    radii = rng.uniform(0.05, 0.2, size=count)
+    cfg = base_config(h, d, (1.6, 1.0, 1.0), 2, 4, 1.0 / 60.0, int(ns.sum()), 1 << 17)
+    scenes = []
+    for k in range(count):
+        box = boxes[k]
+        pos = block(int(ns[k]), d, box, 0.001, seed * 1000 + k)
+        center = (0.75 * box[0], 0.3 * box[1], 0.5 * box[2])
+        grid, origin, cell = sphere_grid(float(radii[k]), center, d)
+        scenes.append(dict(n=int(ns[k]), bounds_min=(0.0, 0.0, 0.0), bounds_max=tuple(float(v) for v in box),
+                           hash_size=1 << 17, pos=pos, vel=np.zeros_like(pos),
+                           sdf=(grid, origin, cell, d / 2.0), radius=float(radii[k]), center=center))
+    return cfg, scenes
 
 
 def c4(seed=0):
