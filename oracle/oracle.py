@@ -121,6 +121,8 @@ def lib():
         L.orc_vorticity.argtypes = [C.POINTER(OrcParams), C.c_uint32, f64p, f64p, f64p, u32p, i32p]
         L.orc_step.argtypes = [C.POINTER(OrcParams), C.c_void_p, C.c_uint32, f64p, f64p, C.c_void_p, C.c_void_p,
                                C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_adjoint_step.argtypes = [C.POINTER(OrcParams), C.c_void_p, C.c_uint32, f64p, f64p, C.c_void_p,
+                                       C.c_void_p, f64p, f64p, f64p, C.c_void_p, C.c_void_p]
         L.orc_kernels.argtypes = [C.POINTER(OrcParams), f64p, C.POINTER(C.c_double), f64p]
         L.orc_neighbor_lists.argtypes = [C.POINTER(OrcParams), C.c_uint32, f64p, u32p, i32p, i32p, C.c_void_p,
                                          C.c_int32]
@@ -227,6 +229,25 @@ def step(params, pos, vel, sdf=None, want=False):
     if want:
         return dict(omega=om, rho=rho, sorted_keys=sk, sorted_ids=ids, table=tab.reshape(-1, 2))
     return None
+
+
+def adjoint_step(params, pos0, vel0, gpos=None, gvel=None, sdf=None):
+    """FP64 reverse-mode derivative of one step (orc_adjoint_step).  Returns
+    (gpos0, gvel0, gt, pos_T, vel_T); gt is the adjoint of the SDF origin
+    offset (translation)."""
+    n = len(pos0)
+    p0 = np.ascontiguousarray(pos0, dtype=np.float64).reshape(-1)
+    v0 = np.ascontiguousarray(vel0, dtype=np.float64).reshape(-1)
+    gp = None if gpos is None else np.ascontiguousarray(gpos, dtype=np.float64).reshape(-1)
+    gv = None if gvel is None else np.ascontiguousarray(gvel, dtype=np.float64).reshape(-1)
+    gp0 = np.zeros(3 * n)
+    gv0 = np.zeros(3 * n)
+    gt = np.zeros(3)
+    pT = np.zeros(3 * n)
+    vT = np.zeros(3 * n)
+    lib().orc_adjoint_step(C.byref(params.p), sdf.ref() if sdf else None, n, p0, v0, _ptr(gp), _ptr(gv), gp0, gv0,
+                           gt, _ptr(pT), _ptr(vT))
+    return gp0.reshape(n, 3), gv0.reshape(n, 3), gt, pT.reshape(n, 3), vT.reshape(n, 3)
 
 
 # ---- reference builds -------------------------------------------------------

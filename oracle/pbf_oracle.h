@@ -119,6 +119,15 @@ void orc_step(const orc_params* p, const orc_sdf* s, uint32_t n, double* pos, do
               double* omega, double* rho, uint32_t* sorted_keys, uint32_t* sorted_ids,
               int32_t* table);
 
+/* Reverse-mode derivative of orc_step (pbf_adjoint.c): from the adjoints of
+ * the final positions/velocities (gpos/gvel, may be NULL = zero) to those of
+ * the initial state (gpos0/gvel0) and of the SDF translation (gt, the origin
+ * offset already applied to s).  pos_out/vel_out (may be NULL) receive the
+ * forward result.  APBF and the interaction force must be off. */
+void orc_adjoint_step(const orc_params* p, const orc_sdf* s, uint32_t n, const double* pos0, const double* vel0,
+                      const double* gpos, const double* gvel, double* gpos0, double* gvel0, double* gt,
+                      double* pos_out, double* vel_out);
+
 /* CS_ContactFilter.glsl:68-83, deterministic (particle order).  Returns the
  * count; out_idx receives the particle ids. */
 uint32_t orc_contact_filter(const orc_sdf* s, uint32_t n, const double* pos, double band,
