@@ -383,6 +383,29 @@ typedef struct pbf_batch_tuning {
 int pbf_batch_autotune(pbf_batch* b, uint32_t trial_steps, pbf_batch_tuning* best, pbf_batch_tuning* results,
                        uint32_t max_results, uint32_t* num_results);
 
+/* ---- differentiable step ----------------------------------------------------
+ * No reference counterpart.  Reverse-mode derivative of one step of a batch
+ * (all substeps x iterations, then vorticity) with respect to the initial
+ * particle positions and velocities and each scene's SDF translation.  The
+ * sort permutation and every discrete choice (neighbour sets, wall and SDF
+ * contacts, clamps) are replayed from the recorded forward, not
+ * differentiated.  Per-substep checkpoints of (x, v) are kept; the backward
+ * recomputes each substep from its checkpoint.  APBF must be off.
+ *
+ * State arrays are n float4 (x, pad) / (v, pad) in the concatenated particle
+ * order; pointers may be device or host memory (unified addressing). */
+/* Translate scene `scene`'s SDF by t (the grid origin moves by t). */
+int pbf_batch_set_sdf_offset(pbf_batch* b, uint32_t scene, const float t[3]);
+int pbf_batch_set_state(pbf_batch* b, const void* pos4, const void* vel4);
+int pbf_batch_get_state(pbf_batch* b, void* pos4, void* vel4);
+/* One step exactly as pbf_batch_step, keeping what the backward needs. */
+int pbf_batch_forward_record(pbf_batch* b);
+/* Adjoint of the recorded step: gpos4/gvel4 (may be null = 0) are dL/d(final
+ * x, v); out_gpos4/out_gvel4 (may be null) receive dL/d(initial x, v), out_gt
+ * (may be null) 3 floats per scene, dL/d(SDF translation).  Synchronous. */
+int pbf_batch_backward(pbf_batch* b, const void* gpos4, const void* gvel4, void* out_gpos4, void* out_gvel4,
+                       float* out_gt);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -62,8 +62,12 @@ __device__ __forceinline__ void masked_walk(const DevParams& P, const int2* __re
 }
 
 // ---- CS_ComputeLambdas.glsl:108-162: returns (x*, lambda), writes rho ----------------------
-__device__ __forceinline__ float4 lambda_particle(const DevParams& P, const int2* __restrict__ table, uint32_t mask,
-                                                  const float4* __restrict__ xin, int s, float& rho_out)
+// The _x form also returns grad C_i / (the scaled sum of spiky gradients)
+// and the denominator sum |grad C|^2 + eps that lambda divides by (the
+// adjoint replays them).
+__device__ __forceinline__ float4 lambda_particle_x(const DevParams& P, const int2* __restrict__ table,
+                                                    uint32_t mask, const float4* __restrict__ xin, int s,
+                                                    float& rho_out, float3& g_out, float& den_out)
 {
     const float4 xi = __ldg(xin + s);
     float rho = P.w0_self, sg = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
@@ -89,7 +93,17 @@ __device__ __forceinline__ float4 lambda_particle(const DevParams& P, const int2
     const float C = fmaxf(rho / P.rho0 - 1.0f, -P.cohesion);
     sg += gx * gx + gy * gy + gz * gz;
     rho_out = rho;
-    return make_float4(xi.x, xi.y, xi.z, -C / (sg + P.eps));
+    g_out = make_float3(gx, gy, gz);
+    den_out = sg + P.eps;
+    return make_float4(xi.x, xi.y, xi.z, -C / den_out);
+}
+
+__device__ __forceinline__ float4 lambda_particle(const DevParams& P, const int2* __restrict__ table, uint32_t mask,
+                                                  const float4* __restrict__ xin, int s, float& rho_out)
+{
+    float3 g;
+    float den;
+    return lambda_particle_x(P, table, mask, xin, s, rho_out, g, den);
 }
 
 // s_corr * (poly6 coefficient form) of CS_ComputeDeltaP.glsl:94-104 added to
@@ -113,8 +127,10 @@ __device__ __forceinline__ float scorr_term(const DevParams& P, float r2)
 }
 
 // ---- CS_ComputeDeltaP.glsl:120-166 + CS_ApplyDeltaP.glsl:80-124: returns (x* + dp, lambda) -----
-__device__ __forceinline__ float4 deltap_particle(const DevParams& P, const int2* __restrict__ table, uint32_t mask,
-                                                  const SdfDev& sdf, const float4* __restrict__ xin, int s)
+// The _x form also returns dp before the 0.5 h clamp.
+__device__ __forceinline__ float4 deltap_particle_x(const DevParams& P, const int2* __restrict__ table,
+                                                    uint32_t mask, const SdfDev& sdf,
+                                                    const float4* __restrict__ xin, int s, float3& dp_raw)
 {
     const float4 xi = __ldg(xin + s);
     const float li = xi.w;
@@ -136,6 +152,7 @@ __device__ __forceinline__ float4 deltap_particle(const DevParams& P, const int2
     dx *= P.inv_rho0;
     dy *= P.inv_rho0;
     dz *= P.inv_rho0;
+    dp_raw = make_float3(dx, dy, dz);
     const float l2 = dx * dx + dy * dy + dz * dz;
     if (l2 > P.max_dp * P.max_dp) {
         const float sc = P.max_dp * rsqrtf(l2);
@@ -149,6 +166,13 @@ __device__ __forceinline__ float4 deltap_particle(const DevParams& P, const int2
         sdf_project(sdf, p, nrm);
     }
     return make_float4(p.x, p.y, p.z, li);
+}
+
+__device__ __forceinline__ float4 deltap_particle(const DevParams& P, const int2* __restrict__ table, uint32_t mask,
+                                                  const SdfDev& sdf, const float4* __restrict__ xin, int s)
+{
+    float3 dp;
+    return deltap_particle_x(P, table, mask, sdf, xin, s, dp);
 }
 
 // ---- CS_Integrate.glsl:135-280 (pre-dispatch neighbour velocities) ---------------------------

@@ -78,6 +78,7 @@ pbf_batch::~pbf_batch()
     bfree(mcode); bfree(mka); bfree(mia); bfree(mkb); bfree(mib);
     bfree(sx[0]); bfree(sx[1]); bfree(sv); bfree(sx0); bfree(somega); bfree(rho); bfree(lod);
     bfree(save_pos); bfree(save_vel);
+    ad_free();
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -87,6 +88,12 @@ void pbf_batch::invalidate_graph()
     if (graph) cudaGraphDestroy(graph);
     graph_exec = nullptr;
     graph = nullptr;
+    if (rec_exec) cudaGraphExecDestroy(rec_exec);
+    if (rec_graph) cudaGraphDestroy(rec_graph);
+    if (bwd_exec) cudaGraphExecDestroy(bwd_exec);
+    if (bwd_graph) cudaGraphDestroy(bwd_graph);
+    rec_exec = bwd_exec = nullptr;
+    rec_graph = bwd_graph = nullptr;
 }
 
 // Shared constants; the walls, hash mask and SDF of DevParams are unused
@@ -163,9 +170,9 @@ int pbf_batch::upload_scenes()
             d.sdf.dx = s.dims[0];
             d.sdf.dy = s.dims[1];
             d.sdf.dz = s.dims[2];
-            d.sdf.ox = s.origin[0];
-            d.sdf.oy = s.origin[1];
-            d.sdf.oz = s.origin[2];
+            d.sdf.ox = s.origin[0] + s.sdf_offset[0];
+            d.sdf.oy = s.origin[1] + s.sdf_offset[1];
+            d.sdf.oz = s.origin[2] + s.sdf_offset[2];
             d.sdf.cell = s.cell;
             d.sdf.inv_cell = 1.0f / s.cell;
             d.sdf.padding = s.sdf_padding;
@@ -186,34 +193,47 @@ int pbf_batch::upload_scenes()
     return PBF_OK;
 }
 
-int pbf_batch::step_body()
+// One substep from (src_pos, src_vel) to (dst_pos, dst_vel); the sorted
+// arrays, table and processing order are left describing this substep.
+int pbf_batch::substep_body(const float4* src_pos, const float4* src_vel, float4* dst_pos, float4* dst_vel)
 {
     const DevParams P = dev_params();
     const int sms = num_sms;
     BatchLaunch L = launch;
     L.sms = sms;
     const uint32_t max_iter = derived.enable_apbf ? derived.max_lod : cfg.solver_iterations;
+    launch_b_predict(P, scenes_dev, scene_of, src_pos, src_vel, keys, sms, stream);
+    launch_radix_sort(n, key_bits, keys, ka, ia, kb, ib, hist, totals, &skeys, &ids, stream, &launches);
+    BCK(cudaMemsetAsync(table, 0xFF, sizeof(int2) * (size_t)table_size, stream));
+    launch_build_table(n, skeys, table, sms, stream);
+    launch_b_reorder(P, scenes_dev, scene_of, ids, src_pos, src_vel, sx[0], sv, sx0, lod, morton ? mcode : nullptr,
+                     mbits, sms, stream);
+    launches += 3;
+    order = nullptr;
+    if (morton) {
+        uint32_t* msorted = nullptr;
+        launch_radix_sort(n, order_bits, mcode, mka, mia, mkb, mib, hist, totals, &msorted, &order, stream,
+                          &launches);
+    }
+    for (uint32_t it = 1; it <= max_iter; ++it) {
+        launch_b_lambda(P, L, scenes_dev, scene_of, sx[0], sx[1], rho, table, lod, it, order, stream);
+        launch_b_deltap(P, L, scenes_dev, scene_of, sx[1], sx[0], table, lod, it, order, stream);
+        launches += 2;
+    }
+    launch_b_integrate(P, L, scenes_dev, scene_of, sx[0], sv, sx0, somega, ids, dst_pos, dst_vel, table, order,
+                       stream);
+    ++launches;
+    return PBF_OK;
+}
+
+int pbf_batch::step_body()
+{
+    const DevParams P = dev_params();
+    BatchLaunch L = launch;
+    L.sms = num_sms;
     for (uint32_t sub = 0; sub < cfg.substep_iterations; ++sub) {
-        launch_b_predict(P, scenes_dev, scene_of, pos, vel, keys, sms, stream);
-        launch_radix_sort(n, key_bits, keys, ka, ia, kb, ib, hist, totals, &skeys, &ids, stream, &launches);
-        BCK(cudaMemsetAsync(table, 0xFF, sizeof(int2) * (size_t)table_size, stream));
-        launch_build_table(n, skeys, table, sms, stream);
-        launch_b_reorder(P, scenes_dev, scene_of, ids, pos, vel, sx[0], sv, sx0, lod, morton ? mcode : nullptr, mbits,
-                         sms, stream);
-        launches += 3;
-        order = nullptr;
-        if (morton) {
-            uint32_t* msorted = nullptr;
-            launch_radix_sort(n, order_bits, mcode, mka, mia, mkb, mib, hist, totals, &msorted, &order, stream,
-                              &launches);
-        }
-        for (uint32_t it = 1; it <= max_iter; ++it) {
-            launch_b_lambda(P, L, scenes_dev, scene_of, sx[0], sx[1], rho, table, lod, it, order, stream);
-            launch_b_deltap(P, L, scenes_dev, scene_of, sx[1], sx[0], table, lod, it, order, stream);
-            launches += 2;
-        }
-        launch_b_integrate(P, L, scenes_dev, scene_of, sx[0], sv, sx0, somega, ids, pos, vel, table, order, stream);
-        ++launches;
+        const int rc = substep_body(pos, vel, pos, vel);
+        if (rc) return rc;
     }
     if (cfg.enable_vorticity) {
         launch_b_vorticity(P, L, scenes_dev, scene_of, sx0, somega, ids, vel, table, order, stream);

@@ -46,6 +46,28 @@ void launch_b_vorticity(const DevParams& P, const BatchLaunch& L, const SceneDev
                         const uint32_t* order, cudaStream_t st);
 int batch_max_blocks_per_sm(int block);
 
+// ---- k_adjoint.cu ---------------------------------------------------------------------------
+void launch_ad_lambda_rec(const DevParams& P, const SceneDev* scenes, const uint16_t* scene_of, const uint32_t* order,
+                          const int2* table, const float4* xin, float4* xl, float4* auxl, float* rhol, cudaStream_t st);
+void launch_ad_deltap_rec(const DevParams& P, const SceneDev* scenes, const uint16_t* scene_of, const uint32_t* order,
+                          const int2* table, const float4* xl, float4* xout, float4* auxd, cudaStream_t st);
+void launch_ad_vorticity(const DevParams& P, const SceneDev* scenes, const uint16_t* scene_of, const uint32_t* order,
+                         const int2* table, const float4* spos, const float4* somega, const uint32_t* ids,
+                         const float4* velb, float4* posb_s, float4* omb, cudaStream_t st);
+void launch_ad_integrate(const DevParams& P, const SceneDev* scenes, const uint16_t* scene_of, const uint32_t* order,
+                         const int2* table, const float4* xs, const float4* sv, const float4* cp_pos,
+                         const uint32_t* ids, const float4* posb, const float4* velb, const float4* posb_s,
+                         const float4* omb, const float4* somega, float4* gx, float4* gv, float4* x0b, float* tgrad,
+                         cudaStream_t st);
+void launch_ad_deltap(const DevParams& P, const SceneDev* scenes, const uint16_t* scene_of, const uint32_t* order,
+                      const int2* table, const float4* xl, const float4* auxd, const float4* gin, float4* gout,
+                      float* tgrad, cudaStream_t st);
+void launch_ad_lambda(const DevParams& P, const SceneDev* scenes, const uint16_t* scene_of, const uint32_t* order,
+                      const int2* table, const float4* xl, const float4* auxl, const float* rhol, float4* gout,
+                      cudaStream_t st);
+void launch_ad_predict(uint32_t n, float dt, const uint32_t* ids, const float4* gx, const float4* gv,
+                       const float4* x0b, float4* posb, float4* velb, int sms, cudaStream_t st);
+
 }  // namespace pbf
 
 struct pbf_batch {
@@ -68,6 +90,7 @@ struct pbf_batch {
         bool sdf_on = false;
         float sdf_padding = 0.0f;
         bool containment = false;
+        float sdf_offset[3] = {0, 0, 0};  // translation of the SDF (differentiable pose)
     };
     std::vector<Scene> scenes;
     uint32_t n = 0;            // total particles
@@ -105,10 +128,31 @@ struct pbf_batch {
     cudaGraphExec_t graph_exec = nullptr;
     uint64_t graph_launches = 0;
 
+    // adjoint (pbf_adjoint.cu): per-substep checkpoints of the recorded step,
+    // per-iteration recomputation buffers, adjoint accumulators
+    uint32_t ad_subs = 0, ad_iters = 0;
+    bool recorded = false;
+    float4 *cp_pos = nullptr, *cp_vel = nullptr;       // substeps x n, particle order
+    float4 *xl = nullptr, *auxl = nullptr, *auxd = nullptr;  // iterations x n, sorted
+    float* rhol = nullptr;                              // iterations x n
+    float4 *gxa = nullptr, *gxb = nullptr, *gv = nullptr, *x0b = nullptr;  // sorted
+    float4 *pb = nullptr, *vb = nullptr;                // particle order
+    float4 *pbs = nullptr, *omb = nullptr;              // sorted (vorticity reverse)
+    float4 *tpos = nullptr, *tvel = nullptr;            // particle-order scratch of the recompute
+    float* tgrad = nullptr;                             // 4 per scene
+    cudaGraph_t rec_graph = nullptr, bwd_graph = nullptr;
+    cudaGraphExec_t rec_exec = nullptr, bwd_exec = nullptr;
+    uint64_t rec_launches = 0, bwd_launches = 0;
+
     ~pbf_batch();
     pbf::DevParams dev_params() const;
     int upload_scenes();
     void invalidate_graph();
     int step_body();
     int step();
+    int substep_body(const float4* src_pos, const float4* src_vel, float4* dst_pos, float4* dst_vel);
+    int ad_alloc();
+    void ad_free();
+    int record_body();
+    int backward_body();
 };

@@ -483,6 +483,29 @@ class Batch:
 
         return d(best), [d(res[i]) for i in range(cnt.value)]
 
+    # ---- differentiable step (pbf_batch_forward_record / pbf_batch_backward) ----
+    def set_sdf_offset(self, k, t):
+        check(lib().pbf_batch_set_sdf_offset(self._b, int(k), fvec(t)))
+
+    def set_state(self, pos4_ptr, vel4_ptr):
+        """State from n float4 arrays (device or host addresses)."""
+        check(lib().pbf_batch_set_state(self._b, C.c_void_p(pos4_ptr), C.c_void_p(vel4_ptr)))
+
+    def get_state(self, pos4_ptr, vel4_ptr):
+        check(lib().pbf_batch_get_state(self._b, C.c_void_p(pos4_ptr), C.c_void_p(vel4_ptr)))
+
+    def forward_record(self):
+        check(lib().pbf_batch_forward_record(self._b))
+
+    def backward(self, gpos4_ptr, gvel4_ptr, out_gpos4_ptr, out_gvel4_ptr):
+        """Adjoint of the recorded step; returns dL/d(SDF translation) as a
+        (num_scenes, 3) float32 array."""
+        gt = np.zeros((self.num_scenes, 3), np.float32)
+        check(lib().pbf_batch_backward(self._b, C.c_void_p(gpos4_ptr), C.c_void_p(gvel4_ptr),
+                                       C.c_void_p(out_gpos4_ptr), C.c_void_p(out_gvel4_ptr),
+                                       gt.ctypes.data_as(C.POINTER(C.c_float))))
+        return gt
+
 
 def sort_keys(keys, key_bits):
     """Stable (key, id) radix sort on the GPU (the CS_Radix* contract)."""

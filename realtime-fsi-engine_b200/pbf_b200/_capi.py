@@ -170,6 +170,12 @@ SIGNATURES = [
     ("pbf_batch_set_option", C.c_int, [vp, C.c_int, C.c_int]),
     ("pbf_batch_get_option", C.c_int, [vp, C.c_int, P(C.c_int)]),
     ("pbf_batch_autotune", C.c_int, [vp, u32, vp, vp, u32, P(u32)]),
+    # differentiable step
+    ("pbf_batch_set_sdf_offset", C.c_int, [vp, u32, P(C.c_float)]),
+    ("pbf_batch_set_state", C.c_int, [vp, vp, vp]),
+    ("pbf_batch_get_state", C.c_int, [vp, vp, vp]),
+    ("pbf_batch_forward_record", C.c_int, [vp]),
+    ("pbf_batch_backward", C.c_int, [vp, vp, vp, vp, vp, P(C.c_float)]),
 ]
 
 _lib = None

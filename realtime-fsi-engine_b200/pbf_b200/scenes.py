@@ -239,9 +239,16 @@ def c3(seed=7, count=64, sizes=None):
 
 
 def c4(seed=0):
+    """C4: the C0 block with 16 substeps x 4 iterations in one step; target =
+    lattice + (0.3, 0, 0.1) + N(0, 0.01) (seed 1); a sphere obstacle r=0.15
+    centred at (0.78, 0.32, 0.32), touching the block's +x face so that its
+    translation has a gradient within the step.  Returns cfg, pos, vel,
+    target, sphere and the sphere's SDF grid (grid, origin, cell, padding)."""
     cfg, pos, vel = c0(32, seed)
     cfg.substep_iterations = 16
     rng = np.random.default_rng(1)
     target = pos.astype(np.float64) + np.array([0.3, 0.0, 0.1]) + rng.normal(0.0, 0.01, size=pos.shape)
-    sphere = dict(radius=0.15, center=(1.0, 0.15, 0.5))
-    return cfg, pos, vel, target, sphere
+    sphere = dict(radius=0.15, center=(0.78, 0.32, 0.32))
+    d = 0.02
+    grid, origin, cell = sphere_grid(sphere["radius"], sphere["center"], d)
+    return cfg, pos, vel, target, sphere, (grid, origin, cell, d / 2.0)

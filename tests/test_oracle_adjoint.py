@@ -14,45 +14,11 @@ roundoff far below the tolerance).  With s_corr on (k = 0.1 at unit mass)
 the Jacobi iterations amplify perturbations by orders of magnitude per
 substep; those cases use one substep.
 """
-import ctypes as C
-
 import numpy as np
 import pytest
 
 import oracle as O
-from pbf_b200 import scenes as S
-
-
-def setup(nside=8, subs=1, iters=1, sdf=True, scorr=True, visc=True, vort=True, seed=0):
-    d, h = 0.02, 0.04
-    n = nside ** 3
-    cfg = S.base_config(h, d, (0.5, 0.5, 0.5), subs, iters, 1 / 60, n, 1 << 12)
-    cfg.enable_scorr, cfg.enable_viscosity, cfg.enable_vorticity = int(scorr), int(visc), int(vort)
-    pos = S.lattice(nside, nside, nside, d, (0.1, 0.05, 0.1), 0.001, seed).astype(np.float64)
-    rng = np.random.default_rng(seed + 1)
-    vel = rng.normal(0, 0.3, pos.shape)
-    oc = O.FluidConfig()
-    C.memmove(C.byref(oc), C.byref(cfg), C.sizeof(oc))
-    P = O.Params(oc)
-    grid = None
-    if sdf:
-        g, origin, cell = S.sphere_grid(0.08, (0.2, 0.12, 0.2), d)
-        grid = (g, origin, cell, d / 2)
-    target = pos + np.array([0.05, 0, 0.02]) + rng.normal(0, 0.01, pos.shape)
-    return P, pos, vel, grid, target
-
-
-def mk_sdf(grid, t):
-    if grid is None:
-        return None
-    g, o, c, pad = grid
-    return O.Sdf(g, np.asarray(o) + t, c, padding=pad)
-
-
-def loss(P, pos, vel, grid, t, target):
-    p, v = pos.copy(), vel.copy()
-    O.step(P, p, v, sdf=mk_sdf(grid, t))
-    return ((p - target) ** 2).sum(1).mean(), p, v
+from adjoint_cases import loss, mk_sdf, setup
 
 
 CASES = [
@@ -67,7 +33,7 @@ CASES = [
 
 @pytest.mark.parametrize("kw,eps,tol", CASES)
 def test_adjoint_matches_central_differences(kw, eps, tol):
-    P, pos, vel, grid, target = setup(**kw)
+    _, P, pos, vel, grid, target = setup(**kw)
     n = len(pos)
     t0 = np.zeros(3)
     L0, pT, vT = loss(P, pos, vel, grid, t0, target)
@@ -96,7 +62,7 @@ def test_adjoint_matches_central_differences(kw, eps, tol):
 def test_velocity_loss_adjoint():
     """Adjoint of a loss on the final velocities (exercises the velocity
     chain of integrate and the vorticity pass)."""
-    P, pos, vel, grid, target = setup(subs=2, iters=2, sdf=True, scorr=False)
+    _, P, pos, vel, grid, target = setup(subs=2, iters=2, sdf=True, scorr=False)
     n = len(pos)
     t0 = np.zeros(3)
     wv = np.random.default_rng(9).normal(size=vel.shape)
