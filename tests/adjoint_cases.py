@@ -13,13 +13,15 @@ import oracle as O
 from pbf_b200 import scenes as S
 
 
-def setup(nside=8, subs=1, iters=1, sdf=True, scorr=True, visc=True, vort=True, seed=0):
+def setup(nside=8, subs=1, iters=1, sdf=True, scorr=True, visc=True, vort=True, seed=0, cohesion=None):
     """Returns (cfg, oracle params, pos, vel, grid, target); grid is
     (dist, origin, cell, padding) or None."""
     d, h = 0.02, 0.04
     n = nside ** 3
     cfg = S.base_config(h, d, (0.5, 0.5, 0.5), subs, iters, 1 / 60, n, 1 << 12)
     cfg.enable_scorr, cfg.enable_viscosity, cfg.enable_vorticity = int(scorr), int(visc), int(vort)
+    if cohesion is not None:
+        cfg.cohesion_strength = cohesion
     pos = S.lattice(nside, nside, nside, d, (0.1, 0.05, 0.1), 0.001, seed).astype(np.float64)
     rng = np.random.default_rng(seed + 1)
     vel = rng.normal(0, 0.3, pos.shape)
