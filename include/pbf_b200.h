@@ -297,10 +297,23 @@ int pbf_set_use_graph(pbf_handle* h, int on);
  *                          buckets of each 256-particle block staged once in
  *                          shared memory (falls back to global reads when a
  *                          block's buckets exceed the stage); 0: hash order.
+ *                          6: Morton-labelled data and per-substep neighbour
+ *                          lists built in the first lambda pass with a skin
+ *                          (PBF_OPT_LIST_SKIN); later passes walk the list
+ *                          where it provably yields the bucket walk's hits
+ *                          and walk the buckets elsewhere (APBF runs mode 4).
  *                          Every mode gives the same results up to FP32
- *                          contraction differences. */
+ *                          contraction differences.
+ *   PBF_OPT_LIST_SKIN      mode 6 list reach beyond h, in 1/1000 h (default 100). */
 #define PBF_OPT_SPATIAL_ORDER 1
+#define PBF_OPT_LIST_SKIN 2
 int pbf_set_option(pbf_handle* h, int option, int value);
+
+/* Mode 6 statistics of the last substep, summed over its passes: particles
+ * that walked all 27 buckets instead of their list (moved more than skin/2
+ * or changed cell), marked buckets walked in full from a list, and buckets
+ * marked because one of their particles moved more than skin/2. */
+int pbf_list_stats(pbf_handle* h, uint32_t* full_walks, uint32_t* bucket_walks, uint32_t* marked_buckets);
 
 /* ---- health ------------------------------------------------------------- */
 /* Scan committed state for NaN/Inf; *bad receives the count (0 = healthy). */

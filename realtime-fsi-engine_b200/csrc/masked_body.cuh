@@ -1,17 +1,20 @@
 // masked_body.cuh — per-particle bodies of the neighbour passes, shared by
-// the single-scene kernels (k_masked.cu) and the multi-scene kernels
-// (k_batch.cu) so that both run the same arithmetic on every pair.
+// the single-scene kernels (k_masked.cu, k_list.cu), the multi-scene kernels
+// (k_batch.cu) and the adjoint's recording passes (k_adjoint.cu), so that
+// all of them run the same arithmetic on every pair.
 //
-// Each function takes the scene's bucket table (already offset to the
-// scene's first bucket), its hash mask and, where the pass needs them, the
-// scene's walls and SDF; everything else comes from DevParams.
+// Each pass is a `*_core` function parameterised by a walker: walk(hit, body)
+// calls body(k) for every candidate k with hit(r^2) true, in the reference's
+// visiting order (CS_ComputeLambdas.glsl:126-150: 27 hashed buckets, z outer,
+// x inner, bucket contents in sorted order, colliding buckets once per
+// neighbour cell), where k indexes the position array X the core reads
+// neighbours from.  Two walkers exist: masked_walk below (the hashed buckets
+// themselves) and the neighbour-list walk of k_list.cu (the same candidate
+// sequence, pre-filtered).
 //
-// Walk: for each of the particle's 27 buckets (CS_ComputeLambdas.glsl:126-150,
-// z outer, x inner), up to 8 candidates are loaded with independent
-// predicated loads and reduced to an 8-bit mask of in-range pairs; the body
-// then runs for the set bits in candidate order.  The candidate multiset,
-// its per-bucket order and each pair's arithmetic match the sequential loop
-// of the reference, so sums are accumulated in the same order as there.
+// masked_walk: for each bucket, up to 8 candidates are loaded with
+// independent predicated loads and reduced to an 8-bit mask of hits; the
+// body then runs for the set bits in candidate order.
 #pragma once
 
 #include "pbf_internal.cuh"
@@ -61,32 +64,45 @@ __device__ __forceinline__ void masked_walk(const DevParams& P, const int2* __re
     }
 }
 
-// ---- CS_ComputeLambdas.glsl:108-162: returns (x*, lambda), writes rho ----------------------
-// The _x form also returns grad C_i / (the scaled sum of spiky gradients)
-// and the denominator sum |grad C|^2 + eps that lambda divides by (the
-// adjoint replays them).
-__device__ __forceinline__ float4 lambda_particle_x(const DevParams& P, const int2* __restrict__ table,
-                                                    uint32_t mask, const float4* __restrict__ xin, int s,
-                                                    float& rho_out, float3& g_out, float& den_out)
+// Walker over the hashed buckets of the sorted arrays (slot k = sorted slot).
+struct HashWalk {
+    const DevParams& P;
+    const int2* table;
+    uint32_t mask;
+    const float4* X;
+    float4 xi;
+    int self;
+    template <class Hit, class Body>
+    __device__ __forceinline__ void operator()(Hit&& hit, Body&& body) const
+    {
+        masked_walk(P, table, mask, X, xi.x, xi.y, xi.z, self, hit, body);
+    }
+};
+
+// ---- CS_ComputeLambdas.glsl:108-162 -----------------------------------------------------------
+// Returns (x*, lambda); also rho, grad C_i (the scaled sum of spiky
+// gradients) and the denominator sum |grad C|^2 + eps that lambda divides by
+// (the adjoint replays them).
+template <class Walk>
+__device__ __forceinline__ float4 lambda_core(const DevParams& P, const float4* __restrict__ X, float4 xi,
+                                              Walk&& walk, float& rho_out, float3& g_out, float& den_out)
 {
-    const float4 xi = __ldg(xin + s);
     float rho = P.w0_self, sg = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
-    masked_walk(
-        P, table, mask, xin, xi.x, xi.y, xi.z, s, [&](float r2) { return r2 <= P.h2; },
-        [&](int k) {
-            const float4 xj = __ldg(xin + k);
-            const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-            const float r2 = rx * rx + ry * ry + rz * rz;
-            rho += poly6_in(P, r2);
-            if (r2 >= 1e-10f) {
-                const float sc = spiky_scale(P, r2);
-                const float ax = rx * sc, ay = ry * sc, az = rz * sc;
-                sg += (ax * ax + ay * ay + az * az) * P.inv_rho0_sq;
-                gx += ax;
-                gy += ay;
-                gz += az;
-            }
-        });
+    walk([&](float r2) { return r2 <= P.h2; },
+         [&](int k) {
+             const float4 xj = __ldg(X + k);
+             const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+             const float r2 = rx * rx + ry * ry + rz * rz;
+             rho += poly6_in(P, r2);
+             if (r2 >= 1e-10f) {
+                 const float sc = spiky_scale(P, r2);
+                 const float ax = rx * sc, ay = ry * sc, az = rz * sc;
+                 sg += (ax * ax + ay * ay + az * az) * P.inv_rho0_sq;
+                 gx += ax;
+                 gy += ay;
+                 gz += az;
+             }
+         });
     gx *= P.inv_rho0;
     gy *= P.inv_rho0;
     gz *= P.inv_rho0;
@@ -96,6 +112,14 @@ __device__ __forceinline__ float4 lambda_particle_x(const DevParams& P, const in
     g_out = make_float3(gx, gy, gz);
     den_out = sg + P.eps;
     return make_float4(xi.x, xi.y, xi.z, -C / den_out);
+}
+
+__device__ __forceinline__ float4 lambda_particle_x(const DevParams& P, const int2* __restrict__ table,
+                                                    uint32_t mask, const float4* __restrict__ xin, int s,
+                                                    float& rho_out, float3& g_out, float& den_out)
+{
+    const float4 xi = __ldg(xin + s);
+    return lambda_core(P, xin, xi, HashWalk{P, table, mask, xin, xi, s}, rho_out, g_out, den_out);
 }
 
 __device__ __forceinline__ float4 lambda_particle(const DevParams& P, const int2* __restrict__ table, uint32_t mask,
@@ -126,29 +150,27 @@ __device__ __forceinline__ float scorr_term(const DevParams& P, float r2)
     return 0.0f;
 }
 
-// ---- CS_ComputeDeltaP.glsl:120-166 + CS_ApplyDeltaP.glsl:80-124: returns (x* + dp, lambda) -----
-// The _x form also returns dp before the 0.5 h clamp.
-__device__ __forceinline__ float4 deltap_particle_x(const DevParams& P, const int2* __restrict__ table,
-                                                    uint32_t mask, const SdfDev& sdf,
-                                                    const float4* __restrict__ xin, int s, float3& dp_raw)
+// ---- CS_ComputeDeltaP.glsl:120-166 + CS_ApplyDeltaP.glsl:80-124 --------------------------------
+// Returns (x* + dp, lambda); dp_raw = dp before the 0.5 h clamp.
+template <class Walk>
+__device__ __forceinline__ float4 deltap_core(const DevParams& P, const SdfDev& sdf, const float4* __restrict__ X,
+                                              float4 xi, Walk&& walk, float3& dp_raw)
 {
-    const float4 xi = __ldg(xin + s);
     const float li = xi.w;
     float dx = 0.f, dy = 0.f, dz = 0.f;
-    masked_walk(
-        P, table, mask, xin, xi.x, xi.y, xi.z, s, [&](float r2) { return r2 <= P.h2 && r2 >= 1e-10f; },
-        [&](int k) {
-            const float4 xj = __ldg(xin + k);
-            const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-            const float r2 = rx * rx + ry * ry + rz * rz;
-            const float sc = spiky_scale(P, r2);
-            float f = li + xj.w;
-            if (P.scorr) f += scorr_term(P, r2);
-            const float g = sc * f;
-            dx += rx * g;
-            dy += ry * g;
-            dz += rz * g;
-        });
+    walk([&](float r2) { return r2 <= P.h2 && r2 >= 1e-10f; },
+         [&](int k) {
+             const float4 xj = __ldg(X + k);
+             const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+             const float r2 = rx * rx + ry * ry + rz * rz;
+             const float sc = spiky_scale(P, r2);
+             float f = li + xj.w;
+             if (P.scorr) f += scorr_term(P, r2);
+             const float g = sc * f;
+             dx += rx * g;
+             dy += ry * g;
+             dz += rz * g;
+         });
     dx *= P.inv_rho0;
     dy *= P.inv_rho0;
     dz *= P.inv_rho0;
@@ -168,6 +190,14 @@ __device__ __forceinline__ float4 deltap_particle_x(const DevParams& P, const in
     return make_float4(p.x, p.y, p.z, li);
 }
 
+__device__ __forceinline__ float4 deltap_particle_x(const DevParams& P, const int2* __restrict__ table,
+                                                    uint32_t mask, const SdfDev& sdf,
+                                                    const float4* __restrict__ xin, int s, float3& dp_raw)
+{
+    const float4 xi = __ldg(xin + s);
+    return deltap_core(P, sdf, xin, xi, HashWalk{P, table, mask, xin, xi, s}, dp_raw);
+}
+
 __device__ __forceinline__ float4 deltap_particle(const DevParams& P, const int2* __restrict__ table, uint32_t mask,
                                                   const SdfDev& sdf, const float4* __restrict__ xin, int s)
 {
@@ -176,43 +206,39 @@ __device__ __forceinline__ float4 deltap_particle(const DevParams& P, const int2
 }
 
 // ---- CS_Integrate.glsl:135-280 (pre-dispatch neighbour velocities) ---------------------------
-// Commits x and v of slot s: writes pos/vel at the particle id, sx0[s] = x
-// and somega[s] = (omega, |omega|).
-__device__ __forceinline__ void integrate_particle(const DevParams& P, const int2* __restrict__ table, uint32_t mask,
-                                                   const float* bmin, const float* bmax, const SdfDev& sdf,
-                                                   const float4* __restrict__ xs, const float4* __restrict__ sv,
-                                                   float4* __restrict__ sx0, float4* __restrict__ somega,
-                                                   const uint32_t* __restrict__ ids, float4* __restrict__ pos,
-                                                   float4* __restrict__ vel, int s)
+// From x* (x4), the predicted velocity v0, the substep start p0 and the
+// neighbours' (X, V): the committed position xo (w = p0.w), velocity vo
+// (w = v0.w) and, when vorticity is on, omega4 = (omega, |omega|).
+template <class Walk>
+__device__ __forceinline__ void integrate_core(const DevParams& P, const float* bmin, const float* bmax,
+                                               const SdfDev& sdf, const float4* __restrict__ X,
+                                               const float4* __restrict__ V, float4 x4, float4 v0, float4 p0,
+                                               Walk&& walk, float4& xo, float4& vo, float4& omega4)
 {
-    const float4 x4 = __ldg(xs + s);
-    const float4 v0 = __ldg(sv + s);
     float fx = 0.f, fy = 0.f, fz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
     if (P.visc_on || P.vort_on) {
-        masked_walk(
-            P, table, mask, xs, x4.x, x4.y, x4.z, s, [&](float r2) { return r2 <= P.h2; },
-            [&](int k) {
-                const float4 xj = __ldg(xs + k);
-                const float rx = x4.x - xj.x, ry = x4.y - xj.y, rz = x4.z - xj.z;
-                const float r2 = rx * rx + ry * ry + rz * rz;
-                const float4 vj = __ldg(sv + k);
-                const float ux = vj.x - v0.x, uy = vj.y - v0.y, uz = vj.z - v0.z;
-                if (P.visc_on) {
-                    const float w = poly6_in(P, r2) * P.inv_rho0;
-                    fx += ux * w;
-                    fy += uy * w;
-                    fz += uz * w;
-                }
-                if (P.vort_on && r2 >= 1e-10f) {
-                    const float sc = spiky_scale(P, r2);
-                    const float ax = rx * sc, ay = ry * sc, az = rz * sc;
-                    cx += uy * az - uz * ay;
-                    cy += uz * ax - ux * az;
-                    cz += ux * ay - uy * ax;
-                }
-            });
+        walk([&](float r2) { return r2 <= P.h2; },
+             [&](int k) {
+                 const float4 xj = __ldg(X + k);
+                 const float rx = x4.x - xj.x, ry = x4.y - xj.y, rz = x4.z - xj.z;
+                 const float r2 = rx * rx + ry * ry + rz * rz;
+                 const float4 vj = __ldg(V + k);
+                 const float ux = vj.x - v0.x, uy = vj.y - v0.y, uz = vj.z - v0.z;
+                 if (P.visc_on) {
+                     const float w = poly6_in(P, r2) * P.inv_rho0;
+                     fx += ux * w;
+                     fy += uy * w;
+                     fz += uz * w;
+                 }
+                 if (P.vort_on && r2 >= 1e-10f) {
+                     const float sc = spiky_scale(P, r2);
+                     const float ax = rx * sc, ay = ry * sc, az = rz * sc;
+                     cx += uy * az - uz * ay;
+                     cy += uz * ax - ux * az;
+                     cz += ux * ay - uy * ax;
+                 }
+             });
     }
-    const float4 p0 = sx0[s];
     float3 x = make_float3(x4.x, x4.y, x4.z);
     float vdx = 0.f, vdy = 0.f, vdz = 0.f;
     if (P.visc_on) {
@@ -222,7 +248,7 @@ __device__ __forceinline__ void integrate_particle(const DevParams& P, const int
     }
     if (P.vort_on) {
         const float ox = cx * P.inv_rho0, oy = cy * P.inv_rho0, oz = cz * P.inv_rho0;
-        somega[s] = make_float4(ox, oy, oz, sqrtf(ox * ox + oy * oy + oz * oz));
+        omega4 = make_float4(ox, oy, oz, sqrtf(ox * ox + oy * oy + oz * oz));
     }
     bool colx = false, coly = false, colz = false;
     if (x.x <= bmin[0]) { x.x = bmin[0]; colx = true; }
@@ -253,45 +279,74 @@ __device__ __forceinline__ void integrate_particle(const DevParams& P, const int
         vy -= vn * nrm.y;
         vz -= vn * nrm.z;
     }
+    xo = make_float4(x.x, x.y, x.z, p0.w);
+    vo = make_float4(vx, vy, vz, v0.w);
+}
+
+// Commits x and v of slot s: writes pos/vel at the particle id, sx0[s] = x
+// and somega[s] = (omega, |omega|).
+__device__ __forceinline__ void integrate_particle(const DevParams& P, const int2* __restrict__ table, uint32_t mask,
+                                                   const float* bmin, const float* bmax, const SdfDev& sdf,
+                                                   const float4* __restrict__ xs, const float4* __restrict__ sv,
+                                                   float4* __restrict__ sx0, float4* __restrict__ somega,
+                                                   const uint32_t* __restrict__ ids, float4* __restrict__ pos,
+                                                   float4* __restrict__ vel, int s)
+{
+    const float4 x4 = __ldg(xs + s);
+    const float4 v0 = __ldg(sv + s);
+    const float4 p0 = sx0[s];
+    float4 xo, vo, om;
+    integrate_core(P, bmin, bmax, sdf, xs, sv, x4, v0, p0, HashWalk{P, table, mask, xs, x4, s}, xo, vo, om);
+    if (P.vort_on) somega[s] = om;
     const uint32_t id = __ldg(ids + s);
-    const float4 xo = make_float4(x.x, x.y, x.z, p0.w);
     pos[id] = xo;
-    vel[id] = make_float4(vx, vy, vz, v0.w);
+    vel[id] = vo;
     sx0[s] = xo;
 }
 
 // ---- CS_VorticityConfinement.glsl:133-167 (pass 1) ----------------------------------------------
+// Velocity increment eps (N x omega_i) dt of a particle at xi with vorticity
+// w; returns false when |eta| < 1e-6 (no change).
+template <class Walk>
+__device__ __forceinline__ bool vorticity_core(const DevParams& P, const float4* __restrict__ X,
+                                               const float4* __restrict__ OM, float4 xi, float4 w, Walk&& walk,
+                                               float3& dv)
+{
+    float ex = 0.f, ey = 0.f, ez = 0.f;
+    walk([&](float r2) { return r2 <= P.h2 && r2 >= 1e-10f; },
+         [&](int k) {
+             const float4 xj = __ldg(X + k);
+             const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+             const float r2 = rx * rx + ry * ry + rz * rz;
+             const float sc = spiky_scale(P, r2) * __ldg(&OM[k].w);
+             ex += rx * sc;
+             ey += ry * sc;
+             ez += rz * sc;
+         });
+    ex *= P.inv_rho0;
+    ey *= P.inv_rho0;
+    ez *= P.inv_rho0;
+    const float el = sqrtf(ex * ex + ey * ey + ez * ez);
+    if (el < 1e-6f) return false;
+    const float nx = ex / el, ny = ey / el, nz = ez / el;
+    const float crx = ny * w.z - nz * w.y, cry = nz * w.x - nx * w.z, crz = nx * w.y - ny * w.x;
+    dv = make_float3(P.vort_eps * crx * P.dt, P.vort_eps * cry * P.dt, P.vort_eps * crz * P.dt);
+    return true;
+}
+
 __device__ __forceinline__ void vorticity_particle(const DevParams& P, const int2* __restrict__ table, uint32_t mask,
                                                    const float4* __restrict__ spos,
                                                    const float4* __restrict__ somega,
                                                    const uint32_t* __restrict__ ids, float4* __restrict__ vel, int s)
 {
     const float4 xi = __ldg(spos + s);
-    float ex = 0.f, ey = 0.f, ez = 0.f;
-    masked_walk(
-        P, table, mask, spos, xi.x, xi.y, xi.z, s, [&](float r2) { return r2 <= P.h2 && r2 >= 1e-10f; },
-        [&](int k) {
-            const float4 xj = __ldg(spos + k);
-            const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-            const float r2 = rx * rx + ry * ry + rz * rz;
-            const float sc = spiky_scale(P, r2) * __ldg(&somega[k].w);
-            ex += rx * sc;
-            ey += ry * sc;
-            ez += rz * sc;
-        });
-    ex *= P.inv_rho0;
-    ey *= P.inv_rho0;
-    ez *= P.inv_rho0;
-    const float el = sqrtf(ex * ex + ey * ey + ez * ez);
-    if (el < 1e-6f) return;
-    const float nx = ex / el, ny = ey / el, nz = ez / el;
-    const float4 w = __ldg(somega + s);
-    const float crx = ny * w.z - nz * w.y, cry = nz * w.x - nx * w.z, crz = nx * w.y - ny * w.x;
+    float3 dv;
+    if (!vorticity_core(P, spos, somega, xi, __ldg(somega + s), HashWalk{P, table, mask, spos, xi, s}, dv)) return;
     const uint32_t id = __ldg(ids + s);
     float4 v = vel[id];
-    v.x += P.vort_eps * crx * P.dt;
-    v.y += P.vort_eps * cry * P.dt;
-    v.z += P.vort_eps * crz * P.dt;
+    v.x += dv.x;
+    v.y += dv.y;
+    v.z += dv.z;
     vel[id] = v;
 }
 

@@ -315,6 +315,8 @@ pbf_handle::~pbf_handle()
     dfree(mcode); dfree(mka); dfree(mia); dfree(mkb); dfree(mib); dfree(run_starts); dfree(run_blocks); dfree(ka); dfree(ia); dfree(kb); dfree(ib);
     dfree(sx[0]); dfree(sx[1]); dfree(sv); dfree(sx0); dfree(somega); dfree(rho); dfree(lod);
     dfree(hist); dfree(totals); dfree(table); dfree(cand); dfree(ct_counts); dfree(scalars);
+    dfree(lx[0]); dfree(lx[1]); dfree(lxb); dfree(lv); dfree(lx0); dfree(lom); dfree(lrho);
+    dfree(lid); dfree(lkey); dfree(inv); dfree(list); dfree(lcnt); dfree(lstats); dfree(fastb);
     dfree(grid); dfree(slab_min);
     mesh_free();
     if (stream) cudaStreamDestroy(stream);
@@ -372,11 +374,117 @@ int pbf_handle::prof_collect()
     return PBF_OK;
 }
 
+// ---- neighbour lists (mode 6) ---------------------------------------------------------
+// Mode 6 needs every iteration to run (no APBF skips) and one displacement
+// slot per moving pass; otherwise the handle runs mode 4.
+int pbf_handle::effective_mode() const
+{
+    if (pass_mode == 6 && (derived.enable_apbf || n >= (1u << 27))) return 4;
+    return pass_mode;
+}
+
+int pbf_handle::ensure_list_capacity()
+{
+    int rc;
+    if (cap_list_n < n || !list) {
+        const size_t c = std::max<uint32_t>(n, 1u);
+        if ((rc = dalloc(lx[0], c)) || (rc = dalloc(lx[1], c)) || (rc = dalloc(lxb, c)) || (rc = dalloc(lv, c)) ||
+            (rc = dalloc(lx0, c)) || (rc = dalloc(lom, c)) || (rc = dalloc(lrho, c)) || (rc = dalloc(lid, c)) ||
+            (rc = dalloc(lkey, c)) || (rc = dalloc(inv, c)) || (rc = dalloc(list, c * list_cap)) ||
+            (rc = dalloc(lcnt, c)) || (rc = dalloc(lstats, 4)))
+            return rc;
+        cap_list_n = (uint32_t)c;
+    }
+    if (cap_fast != derived.hash_size || !fastb) {
+        if ((rc = dalloc(fastb, derived.hash_size))) return rc;
+        cap_fast = derived.hash_size;
+    }
+    return PBF_OK;
+}
+
+ListArgs pbf_handle::list_args() const
+{
+    ListArgs A;
+    A.table = table;
+    A.inv = inv;
+    A.list = list;
+    A.cnt = lcnt;
+    A.xb = lxb;
+    A.lkey = lkey;
+    A.fastb = fastb;
+    A.stats = lstats;
+    // margin 1e-4 h absorbs the FP32 rounding of the distances compared
+    const float hs = (0.5f * list_skin - 1e-4f) * derived.h;
+    A.half_skin2 = hs > 0.0f ? hs * hs : 0.0f;
+    return A;
+}
+
+// Sorted-order buffers are kept in label order in mode 6: gather the one
+// asked for back into sorted (hash) order before it is read.
+int pbf_handle::unpermute_for_read(int which)
+{
+    if (!label_space) return PBF_OK;
+    switch (which) {
+    case PBF_BUF_XSTAR:
+        launch_l_unpermute4(n, inv, lx[last_x], sx[last_x], num_sms, stream);
+        break;
+    case PBF_BUF_RHO:
+        launch_l_unpermute1(n, inv, lrho, rho, num_sms, stream);
+        break;
+    case PBF_BUF_OMEGA:
+        launch_l_unpermute4(n, inv, lom, somega, num_sms, stream);
+        break;
+    default:
+        return PBF_OK;
+    }
+    ++launches;
+    CK(cudaStreamSynchronize(stream));
+    return PBF_OK;
+}
+
 // ---- pipeline -------------------------------------------------------------------------
 int pbf_handle::stage(int st, uint32_t iter)
 {
     const DevParams P = dev_params();
     const int sms = num_sms;
+    const int mode = effective_mode();
+    if (mode == 6) {
+        switch (st) {
+        case PBF_STAGE_LAMBDA: {
+            prof_begin(PBF_STAGE_LAMBDA);
+            if (iter <= 1)
+                launch_l_lambda_build(P, table, sx[0], order, inv, lxb, lx[1], lrho, list, lcnt, list_cap,
+                                      (1.0f + list_skin) * derived.h, stream);
+            else
+                launch_l_lambda(P, list_args(), lx[0], lx[1], lrho, stream);
+            ++launches;
+            last_x = 1;
+            prof_end(PBF_STAGE_LAMBDA);
+            return PBF_OK;
+        }
+        case PBF_STAGE_DELTAP:
+            prof_begin(PBF_STAGE_DELTAP);
+            launch_l_deltap(P, list_args(), lx[1], lx[0], stream);
+            ++launches;
+            last_x = 0;
+            prof_end(PBF_STAGE_DELTAP);
+            return PBF_OK;
+        case PBF_STAGE_INTEGRATE:
+            prof_begin(PBF_STAGE_INTEGRATE);
+            launch_l_integrate(P, list_args(), lx[0], lv, lx0, lom, lid, pos, vel, stream);
+            ++launches;
+            prof_end(PBF_STAGE_INTEGRATE);
+            return PBF_OK;
+        case PBF_STAGE_VORTICITY:
+            prof_begin(PBF_STAGE_VORTICITY);
+            launch_l_vorticity(P, list_args(), lx0, lom, lid, vel, stream);
+            ++launches;
+            prof_end(PBF_STAGE_VORTICITY);
+            return PBF_OK;
+        default:
+            break;  // predict, sort, table, reorder: below
+        }
+    }
     switch (st) {
     case PBF_STAGE_PREDICT:
         prof_begin(PBF_STAGE_PREDICT);
@@ -401,26 +509,36 @@ int pbf_handle::stage(int st, uint32_t iter)
         break;
     case PBF_STAGE_REORDER:
         prof_begin(PBF_STAGE_REORDER);
-        launch_reorder(P, ids, pos, vel, sx[0], sv, sx0, lod, pass_mode ? mcode : nullptr, sms, stream);
+        launch_reorder(P, ids, pos, vel, sx[0], sv, sx0, lod, mode ? mcode : nullptr, sms, stream);
         ++launches;
         order = nullptr;
-        if (pass_mode) {
+        if (mode) {
             uint32_t* msorted = nullptr;
             launch_radix_sort(n, 24, mcode, mka, mia, mkb, mib, hist, totals, &msorted, &order, stream, &launches);
-            if (pass_mode == 2) launch_cell_runs(n, msorted, run_blocks, scalars + 2, run_starts, stream, &launches);
+            if (mode == 2) launch_cell_runs(n, msorted, run_blocks, scalars + 2, run_starts, stream, &launches);
+        }
+        label_space = false;
+        if (mode == 6) {
+            int rc = ensure_list_capacity();
+            if (rc) return rc;
+            launch_l_permute(n, order, ids, skeys, sx[0], sv, sx0, lx[0], lxb, lv, lx0, lid, lkey, inv, sms, stream);
+            ++launches;
+            CK(cudaMemsetAsync(fastb, 0, derived.hash_size, stream));
+            CK(cudaMemsetAsync(lstats, 0, sizeof(uint32_t) * 4, stream));
+            label_space = true;
         }
         last_x = 0;
         prof_end(PBF_STAGE_REORDER);
         break;
     case PBF_STAGE_LAMBDA:
         prof_begin(PBF_STAGE_LAMBDA);
-        if (pass_mode == 2)
+        if (mode == 2)
             launch_lambda_coop(P, sx[0], sx[1], rho, table, lod, iter, order, run_starts, scalars + 2, sms, stream);
-        else if (pass_mode == 3)
+        else if (mode == 3)
             launch_lambda_q(P, sx[0], sx[1], rho, table, lod, iter, order, stream);
-        else if (pass_mode == 4)
+        else if (mode == 4)
             launch_lambda_m(P, sx[0], sx[1], rho, table, lod, iter, order, stream);
-        else if (pass_mode == 5)
+        else if (mode == 5)
             launch_lambda_s(P, sx[0], sx[1], rho, table, lod, iter, order, device, stream);
         else
             launch_lambda(P, sx[0], sx[1], rho, table, lod, iter, order, stream);
@@ -430,13 +548,13 @@ int pbf_handle::stage(int st, uint32_t iter)
         break;
     case PBF_STAGE_DELTAP:
         prof_begin(PBF_STAGE_DELTAP);
-        if (pass_mode == 2)
+        if (mode == 2)
             launch_deltap_coop(P, sx[1], sx[0], table, lod, iter, order, run_starts, scalars + 2, sms, stream);
-        else if (pass_mode == 3)
+        else if (mode == 3)
             launch_deltap_q(P, sx[1], sx[0], table, lod, iter, order, stream);
-        else if (pass_mode == 4)
+        else if (mode == 4)
             launch_deltap_m(P, sx[1], sx[0], table, lod, iter, order, stream);
-        else if (pass_mode == 5)
+        else if (mode == 5)
             launch_deltap_s(P, sx[1], sx[0], table, lod, iter, order, device, stream);
         else
             launch_deltap_apply(P, sx[1], sx[0], table, lod, iter, order, stream);
@@ -446,14 +564,14 @@ int pbf_handle::stage(int st, uint32_t iter)
         break;
     case PBF_STAGE_INTEGRATE:
         prof_begin(PBF_STAGE_INTEGRATE);
-        if (pass_mode == 2)
+        if (mode == 2)
             launch_integrate_coop(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, run_starts, scalars + 2,
                                   sms, stream);
-        else if (pass_mode == 3)
+        else if (mode == 3)
             launch_integrate_q(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, stream);
-        else if (pass_mode == 4)
+        else if (mode == 4)
             launch_integrate_m(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, stream);
-        else if (pass_mode == 5)
+        else if (mode == 5)
             launch_integrate_s(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, device, stream);
         else
             launch_integrate(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, stream);
@@ -462,13 +580,13 @@ int pbf_handle::stage(int st, uint32_t iter)
         break;
     case PBF_STAGE_VORTICITY:
         prof_begin(PBF_STAGE_VORTICITY);
-        if (pass_mode == 2)
+        if (mode == 2)
             launch_vorticity_coop(P, sx0, somega, ids, vel, table, order, run_starts, scalars + 2, sms, stream);
-        else if (pass_mode == 3)
+        else if (mode == 3)
             launch_vorticity_q(P, sx0, somega, ids, vel, table, order, stream);
-        else if (pass_mode == 4)
+        else if (mode == 4)
             launch_vorticity_m(P, sx0, somega, ids, vel, table, order, stream);
-        else if (pass_mode == 5)
+        else if (mode == 5)
             launch_vorticity_s(P, sx0, somega, ids, vel, table, order, device, stream);
         else
             launch_vorticity(P, sx0, somega, ids, vel, table, order, stream);
@@ -500,6 +618,10 @@ int pbf_handle::step_body()
 int pbf_handle::step()
 {
     if (n == 0) return PBF_OK;  // PBFluids.cpp:325
+    if (effective_mode() == 6) {
+        const int rc = ensure_list_capacity();  // before any capture
+        if (rc) return rc;
+    }
     const uint64_t gen = sdf_src ? sdf_src->grid_generation : 0;
     if (graph_exec && gen != captured_generation) invalidate_graph();
     if (use_graph) {
@@ -648,6 +770,7 @@ extern "C" int pbf_set_particles(pbf_handle* h, const pbf_particle* ps, uint32_t
     CK(cudaStreamSynchronize(h->stream));
     h->invalidate_graph();
     h->n = n;
+    h->label_space = false;
     h->cfg.particle_count = n;  // PBFluids.cpp:117-118
     pbf_derive_params(&h->cfg, h->collision_padding, &h->derived);
     h->contact_count_host = 0;
@@ -707,6 +830,7 @@ extern "C" int pbf_set_particles_device(pbf_handle* h, const void* pos4, const v
         CK(cudaStreamSynchronize(h->stream));
         h->invalidate_graph();
         h->n = n;
+        h->label_space = false;
         h->cfg.particle_count = n;
         pbf_derive_params(&h->cfg, h->collision_padding, &h->derived);
         if (n) {
@@ -904,6 +1028,7 @@ extern "C" int pbf_run_stage(pbf_handle* h, int stage, uint32_t iter)
 static int buffer_info(pbf_handle* h, int which, void** p, size_t* bytes)
 {
     const size_t n = h->n;
+    if (int rc = h->unpermute_for_read(which)) return rc;
     switch (which) {
     case PBF_BUF_KEYS: *p = h->keys; *bytes = 4 * n; break;
     case PBF_BUF_SORTED_KEYS: *p = h->skeys; *bytes = 4 * n; break;
@@ -1045,12 +1170,32 @@ extern "C" int pbf_set_option(pbf_handle* h, int option, int value)
     if (!h) return set_error(PBF_ERR_INVALID, "null handle");
     switch (option) {
     case PBF_OPT_SPATIAL_ORDER:
-        if (value < 0 || value > 5) return set_error(PBF_ERR_INVALID, "spatial order mode %d", value);
+        if (value < 0 || value > 6) return set_error(PBF_ERR_INVALID, "spatial order mode %d", value);
         h->pass_mode = value;
+        h->label_space = false;
+        break;
+    case PBF_OPT_LIST_SKIN:
+        if (value < 1 || value > 1000) return set_error(PBF_ERR_INVALID, "list skin %d not in [1, 1000] (1/1000 h)", value);
+        h->list_skin = (float)value * 1e-3f;
         break;
     default: return set_error(PBF_ERR_INVALID, "unknown option %d", option);
     }
     h->invalidate_graph();
+    return PBF_OK;
+}
+
+extern "C" int pbf_list_stats(pbf_handle* h, uint32_t* full_walks, uint32_t* bucket_walks, uint32_t* marked_buckets)
+{
+    CHECK_HANDLE(h);
+    if (!full_walks || !bucket_walks || !marked_buckets) return set_error(PBF_ERR_INVALID, "null argument");
+    *full_walks = *bucket_walks = *marked_buckets = 0;
+    if (!h->lstats) return PBF_OK;
+    uint32_t d[4];
+    CK(cudaMemcpyAsync(d, h->lstats, sizeof(d), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    *full_walks = d[0];
+    *bucket_walks = d[1];
+    *marked_buckets = d[2];
     return PBF_OK;
 }
 

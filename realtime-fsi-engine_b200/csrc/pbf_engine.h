@@ -49,6 +49,21 @@ struct pbf_handle {
     // cell runs of the Morton order (one warp per run in the cooperative passes)
     uint32_t* run_starts = nullptr;
     uint32_t* run_blocks = nullptr;
+    // mode 6: neighbour lists over Morton-labelled copies of the sorted arrays
+    float4 *lx[2] = {nullptr, nullptr}, *lxb = nullptr, *lv = nullptr, *lx0 = nullptr, *lom = nullptr;
+    float* lrho = nullptr;
+    uint32_t *lid = nullptr, *lkey = nullptr, *inv = nullptr, *list = nullptr, *lcnt = nullptr;
+    uint32_t* lstats = nullptr;  // 4 counters of the last substep
+    uint8_t* fastb = nullptr;    // per bucket (hash size)
+    uint32_t cap_fast = 0;
+    uint32_t cap_list_n = 0;
+    uint32_t list_cap = 64;      // entries per particle
+    float list_skin = 0.1f;      // in units of h
+    bool label_space = false;    // the current substep's state lives in the label arrays
+    int effective_mode() const;
+    int ensure_list_capacity();
+    pbf::ListArgs list_args() const;
+    int unpermute_for_read(int which);
     // sorted order
     float4* sx[2] = {nullptr, nullptr};
     int last_x = 0;

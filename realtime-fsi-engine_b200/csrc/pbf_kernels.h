@@ -83,6 +83,34 @@ void launch_integrate_s(const DevParams& P, const float4* xs, const float4* sv, 
 void launch_vorticity_s(const DevParams& P, const float4* spos, const float4* somega, const uint32_t* ids,
                         float4* vel, const int2* table, const uint32_t* order, int device, cudaStream_t st);
 
+// ---- k_list.cu: neighbour lists with a skin over Morton-labelled data ----------
+struct ListArgs {
+    const int2* table;
+    const uint32_t* inv;   // hash slot -> label
+    const uint32_t* list;  // cap x n, column-major: bucket index << 27 | label
+    const uint32_t* cnt;   // entries per label (0xFFFFFFFF = overflowed)
+    const float4* xb;      // build positions, label order
+    const uint32_t* lkey;  // bucket (predict-time hash) of each label
+    uint8_t* fastb;        // per bucket: holds a particle that moved > skin/2
+    uint32_t* stats;       // [0] full walks, [1] marked-bucket walks, [2] marked buckets
+    float half_skin2;      // (skin/2 - rounding margin)^2
+};
+void launch_l_permute(uint32_t n, const uint32_t* order, const uint32_t* ids, const uint32_t* skeys,
+                      const float4* sx, const float4* sv, const float4* sx0, float4* lx, float4* lxb, float4* lv,
+                      float4* lx0, uint32_t* lid, uint32_t* lkey, uint32_t* inv, int sms, cudaStream_t st);
+void launch_l_lambda_build(const DevParams& P, const int2* table, const float4* sx, const uint32_t* order,
+                           const uint32_t* inv, const float4* lxb, float4* lx_out, float* lrho, uint32_t* list,
+                           uint32_t* cnt, uint32_t cap, float reach, cudaStream_t st);
+void launch_l_lambda(const DevParams& P, const ListArgs& A, const float4* lx_in, float4* lx_out, float* lrho,
+                     cudaStream_t st);
+void launch_l_deltap(const DevParams& P, const ListArgs& A, const float4* lx_in, float4* lx_out, cudaStream_t st);
+void launch_l_integrate(const DevParams& P, const ListArgs& A, const float4* lx, const float4* lv, float4* lx0,
+                        float4* lom, const uint32_t* lid, float4* pos, float4* vel, cudaStream_t st);
+void launch_l_vorticity(const DevParams& P, const ListArgs& A, const float4* lx0, const float4* lom,
+                        const uint32_t* lid, float4* vel, cudaStream_t st);
+void launch_l_unpermute4(uint32_t n, const uint32_t* inv, const float4* src, float4* dst, int sms, cudaStream_t st);
+void launch_l_unpermute1(uint32_t n, const uint32_t* inv, const float* src, float* dst, int sms, cudaStream_t st);
+
 // ---- k_sort.cu ----------------------------------------------------------------
 uint32_t sort_num_tiles(uint32_t n);
 void launch_radix_sort(uint32_t n, uint32_t key_bits, const uint32_t* keys_in, uint32_t* ka, uint32_t* ia,

@@ -355,6 +355,13 @@ class PBFluids:
     def set_option(self, option, value):
         check(lib().pbf_set_option(self._h, int(option), int(value)))
 
+    def list_stats(self):
+        """Mode 6, last substep, summed over passes: (particles that walked
+        all buckets, marked buckets walked in full, buckets marked)."""
+        a, b, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        check(lib().pbf_list_stats(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
     def check_finite(self):
         bad = C.c_uint32()
         rc = lib().pbf_check_finite(self._h, C.byref(bad))

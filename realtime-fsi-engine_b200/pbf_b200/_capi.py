@@ -150,6 +150,7 @@ SIGNATURES = [
     ("pbf_kernel_launches", C.c_int, [vp, P(C.c_uint64)]),
     ("pbf_set_use_graph", C.c_int, [vp, C.c_int]),
     ("pbf_set_option", C.c_int, [vp, C.c_int, C.c_int]),
+    ("pbf_list_stats", C.c_int, [vp, P(u32), P(u32), P(u32)]),
     ("pbf_check_finite", C.c_int, [vp, P(u32)]),
     # batched scenes
     ("pbf_batch_create", C.c_int, [P(FluidConfig), vp, u32, C.c_int, P(vp)]),

@@ -88,7 +88,7 @@ def test_cell_table_bit_exact(have_gpu):
                          [("glsl_stages_scorr.npz", 2), ("glsl_stages_apbf.npz", 2), ("glsl_stages_sdf.npz", 2),
                           ("glsl_stages_plain.npz", 0)] +
                          [(f, 3) for f in STAGE_FIXTURES] + [(f, 4) for f in STAGE_FIXTURES] +
-                         [(f, 5) for f in STAGE_FIXTURES])
+                         [(f, 5) for f in STAGE_FIXTURES] + [(f, 6) for f in STAGE_FIXTURES])
 def test_stages_match_oracle(have_gpu, name, mode):
     z = H.load(name)
     fl, sdf = make_fluid(z, mode)
@@ -325,7 +325,7 @@ def test_cooperative_and_per_thread_passes_agree(have_gpu):
     cfg, pos, vel = scenes.c0(16, seed=4)
     cfg.enable_scorr = 0
     outs = {}
-    for mode in (1, 0, 2, 2, 3, 3, 4, 5, 5):
+    for mode in (1, 0, 2, 2, 3, 3, 4, 5, 5, 6, 6):
         fl = P.PBFluids(cfg)
         fl.set_option(1, mode)
         fl.setParticles(P.make_particles(pos, vel))
@@ -335,6 +335,53 @@ def test_cooperative_and_per_thread_passes_agree(have_gpu):
             assert np.array_equal(outs[mode]["pos"], o["pos"]) and np.array_equal(outs[mode]["vel"], o["vel"])
         outs[mode] = o
     assert np.array_equal(outs[0]["pos"], outs[1]["pos"]) and np.array_equal(outs[0]["vel"], outs[1]["vel"])
-    for m in (2, 3, 4, 5):
+    for m in (2, 3, 4, 5, 6):
         assert np.abs(outs[m]["pos"] - outs[1]["pos"]).max() < 1e-5 * cfg.h
         assert np.abs(outs[m]["vel"] - outs[1]["vel"]).max() < 1e-3
+
+
+def _run_mode(cfg, pos, vel, mode, steps, skin=None):
+    fl = P.PBFluids(cfg)
+    fl.set_option(1, mode)
+    if skin is not None:
+        fl.set_option(2, skin)
+    fl.setParticles(P.make_particles(pos, vel))
+    for _ in range(steps):
+        fl.step()
+    return fl, fl.readbackParticles()
+
+
+@pytest.mark.parametrize("skin", [100, 1, 400])
+def test_neighbour_lists_agree_with_bucket_walk(have_gpu, skin):
+    """Mode 6 (lists with a skin, Morton-labelled data) against mode 4 (the
+    bucket walk) over several steps with s_corr on.  A 0.001 h skin sends
+    nearly every particle back to the bucket walk after the first
+    iteration; 0.4 h lists far more candidates than needed.  The visited
+    pairs and their order are the same, so the trajectories agree to FP32
+    contraction differences."""
+    cfg, pos, vel = scenes.c0(16, seed=6)
+    cfg.particle_count = len(pos)
+    _, a = _run_mode(cfg, pos, vel, 4, 2)
+    fl, b = _run_mode(cfg, pos, vel, 6, 2, skin)
+    assert np.abs(a["pos"] - b["pos"]).max() < 1e-5 * cfg.h
+    assert np.abs(a["vel"] - b["vel"]).max() < 1e-3
+    full, buckets, marked = fl.list_stats()
+    if skin == 1:
+        assert full + buckets > 0
+
+
+def test_neighbour_list_overflow_falls_back(have_gpu):
+    """A dense clump lists more than the 64-entry capacity: those particles
+    walk the buckets in every pass and still match mode 4."""
+    cfg, _, _ = scenes.c0(8)
+    rng = np.random.default_rng(8)
+    pos = rng.uniform(0.05, 0.95, size=(3000, 3)).astype(np.float32) * np.array([1.5, 0.9, 0.9], np.float32)
+    pos[:1000] = pos[:1000] * 0.1 + 0.3
+    vel = rng.uniform(-0.5, 0.5, size=pos.shape).astype(np.float32)
+    cfg.enable_scorr = 0
+    cfg.particle_count = len(pos)
+    _, a = _run_mode(cfg, pos, vel, 4, 1)
+    fl, b = _run_mode(cfg, pos, vel, 6, 1)
+    assert fl.list_stats()[0] > 0
+    assert np.abs(a["pos"] - b["pos"]).max() < 1e-5 * cfg.h
+    assert np.abs(a["vel"] - b["vel"]).max() < 1e-3
