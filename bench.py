@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", type=int, default=4, choices=[0, 1, 2, 3, 4, 5, 6],
+    ap.add_argument("--mode", type=int, default=4, choices=[0, 1, 2, 3, 4, 5, 6, 7],
                     help="neighbour passes: 0 hash order, 1 Morton, 2 Morton cell-cooperative, "
                          "3 Morton with per-lane pair queues, 4 Morton with per-bucket hit masks (default), "
                          "5 Morton cell blocks staged through shared memory")

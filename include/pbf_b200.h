@@ -301,7 +301,10 @@ int pbf_set_use_graph(pbf_handle* h, int on);
  *                          lists built in the first lambda pass with a skin
  *                          (PBF_OPT_LIST_SKIN); later passes walk the list
  *                          where it provably yields the bucket walk's hits
- *                          and walk the buckets elsewhere (APBF runs mode 4).
+ *                          and walk the buckets elsewhere (APBF runs mode 4);
+ *                          7: Morton order, each 256-particle block stages the
+ *                          buckets of its widened cell box in shared memory
+ *                          (dense cell table) and walks them there.
  *                          Every mode gives the same results up to FP32
  *                          contraction differences.
  *   PBF_OPT_LIST_SKIN      mode 6 list reach beyond h, in 1/1000 h (default 100). */

@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(kLThreads) k_l_lambda_build(DevParams P, const
     };
     float rho, den;
     float3 g;
-    lx_out[t] = lambda_core(P, sx, xi, walk, rho, g, den);
+    lx_out[t] = lambda_core(P, GSrc{sx}, xi, walk, rho, g, den);
     lrho[t] = rho;
     cnt[t] = c <= cap ? c : 0xFFFFFFFFu;
 }
@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(kLThreads) k_l_lambda(DevParams P, ListArgs L,
     float rho, den;
     float3 g;
     float4 out;
-    with_walker(P, L, lx_in, xi, t, [&](auto&& walk) { out = lambda_core(P, lx_in, xi, walk, rho, g, den); });
+    with_walker(P, L, lx_in, xi, t, [&](auto&& walk) { out = lambda_core(P, GSrc{lx_in}, xi, walk, rho, g, den); });
     lx_out[t] = out;
     lrho[t] = rho;
 }
@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(kLThreads) k_l_deltap(DevParams P, ListArgs L,
     const float4 xi = __ldg(lx_in + t);
     float3 dp;
     float4 out;
-    with_walker(P, L, lx_in, xi, t, [&](auto&& walk) { out = deltap_core(P, P.sdf, lx_in, xi, walk, dp); });
+    with_walker(P, L, lx_in, xi, t, [&](auto&& walk) { out = deltap_core(P, P.sdf, GSrc{lx_in}, xi, walk, dp); });
     lx_out[t] = out;
     mark_if_fast(L, out, t);
 }
@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(kLThreads) k_l_integrate(DevParams P, ListArgs
     const float4 p0 = lx0[t];
     float4 xo, vo, om;
     with_walker(P, L, lx, x4, t,
-                [&](auto&& walk) { integrate_core(P, P.bmin, P.bmax, P.sdf, lx, lv, x4, v0, p0, walk, xo, vo, om); });
+                [&](auto&& walk) { integrate_core(P, P.bmin, P.bmax, P.sdf, GSrc{lx}, GSrc{lv}, x4, v0, p0, walk, xo, vo, om); });
     if (P.vort_on) lom[t] = om;
     const uint32_t id = __ldg(lid + t);
     pos[id] = xo;
@@ -301,7 +301,7 @@ __global__ void __launch_bounds__(kLThreads) k_l_vorticity(DevParams P, ListArgs
     const float4 xi = __ldg(lx0 + t);
     float3 dv;
     bool any = false;
-    with_walker(P, L, lx0, xi, t, [&](auto&& walk) { any = vorticity_core(P, lx0, lom, xi, __ldg(lom + t), walk, dv); });
+    with_walker(P, L, lx0, xi, t, [&](auto&& walk) { any = vorticity_core(P, GSrc{lx0}, GMag{lom}, xi, __ldg(lom + t), walk, dv); });
     if (!any) return;
     const uint32_t id = __ldg(lid + t);
     float4 v = vel[id];

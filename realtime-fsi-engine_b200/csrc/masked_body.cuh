@@ -64,6 +64,25 @@ __device__ __forceinline__ void masked_walk(const DevParams& P, const int2* __re
     }
 }
 
+// Neighbour data sources of the pass cores: global memory through the
+// read-only path, or plain loads (shared memory).
+struct GSrc {
+    const float4* __restrict__ p;
+    __device__ __forceinline__ float4 operator[](int k) const { return __ldg(p + k); }
+};
+struct GMag {  // |omega| in the w of a float4 (omega, |omega|) array
+    const float4* __restrict__ p;
+    __device__ __forceinline__ float operator[](int k) const { return __ldg(&p[k].w); }
+};
+struct SSrc {
+    const float4* p;
+    __device__ __forceinline__ float4 operator[](int k) const { return p[k]; }
+};
+struct SMagW {  // |omega| staged in the w of a position array
+    const float4* p;
+    __device__ __forceinline__ float operator[](int k) const { return p[k].w; }
+};
+
 // Walker over the hashed buckets of the sorted arrays (slot k = sorted slot).
 struct HashWalk {
     const DevParams& P;
@@ -83,14 +102,14 @@ struct HashWalk {
 // Returns (x*, lambda); also rho, grad C_i (the scaled sum of spiky
 // gradients) and the denominator sum |grad C|^2 + eps that lambda divides by
 // (the adjoint replays them).
-template <class Walk>
-__device__ __forceinline__ float4 lambda_core(const DevParams& P, const float4* __restrict__ X, float4 xi,
-                                              Walk&& walk, float& rho_out, float3& g_out, float& den_out)
+template <class XS, class Walk>
+__device__ __forceinline__ float4 lambda_core(const DevParams& P, XS X, float4 xi, Walk&& walk, float& rho_out,
+                                              float3& g_out, float& den_out)
 {
     float rho = P.w0_self, sg = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
     walk([&](float r2) { return r2 <= P.h2; },
          [&](int k) {
-             const float4 xj = __ldg(X + k);
+             const float4 xj = X[k];
              const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
              const float r2 = rx * rx + ry * ry + rz * rz;
              rho += poly6_in(P, r2);
@@ -119,7 +138,7 @@ __device__ __forceinline__ float4 lambda_particle_x(const DevParams& P, const in
                                                     float& rho_out, float3& g_out, float& den_out)
 {
     const float4 xi = __ldg(xin + s);
-    return lambda_core(P, xin, xi, HashWalk{P, table, mask, xin, xi, s}, rho_out, g_out, den_out);
+    return lambda_core(P, GSrc{xin}, xi, HashWalk{P, table, mask, xin, xi, s}, rho_out, g_out, den_out);
 }
 
 __device__ __forceinline__ float4 lambda_particle(const DevParams& P, const int2* __restrict__ table, uint32_t mask,
@@ -152,15 +171,15 @@ __device__ __forceinline__ float scorr_term(const DevParams& P, float r2)
 
 // ---- CS_ComputeDeltaP.glsl:120-166 + CS_ApplyDeltaP.glsl:80-124 --------------------------------
 // Returns (x* + dp, lambda); dp_raw = dp before the 0.5 h clamp.
-template <class Walk>
-__device__ __forceinline__ float4 deltap_core(const DevParams& P, const SdfDev& sdf, const float4* __restrict__ X,
-                                              float4 xi, Walk&& walk, float3& dp_raw)
+template <class XS, class Walk>
+__device__ __forceinline__ float4 deltap_core(const DevParams& P, const SdfDev& sdf, XS X, float4 xi, Walk&& walk,
+                                              float3& dp_raw)
 {
     const float li = xi.w;
     float dx = 0.f, dy = 0.f, dz = 0.f;
     walk([&](float r2) { return r2 <= P.h2 && r2 >= 1e-10f; },
          [&](int k) {
-             const float4 xj = __ldg(X + k);
+             const float4 xj = X[k];
              const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
              const float r2 = rx * rx + ry * ry + rz * rz;
              const float sc = spiky_scale(P, r2);
@@ -195,7 +214,7 @@ __device__ __forceinline__ float4 deltap_particle_x(const DevParams& P, const in
                                                     const float4* __restrict__ xin, int s, float3& dp_raw)
 {
     const float4 xi = __ldg(xin + s);
-    return deltap_core(P, sdf, xin, xi, HashWalk{P, table, mask, xin, xi, s}, dp_raw);
+    return deltap_core(P, sdf, GSrc{xin}, xi, HashWalk{P, table, mask, xin, xi, s}, dp_raw);
 }
 
 __device__ __forceinline__ float4 deltap_particle(const DevParams& P, const int2* __restrict__ table, uint32_t mask,
@@ -209,20 +228,19 @@ __device__ __forceinline__ float4 deltap_particle(const DevParams& P, const int2
 // From x* (x4), the predicted velocity v0, the substep start p0 and the
 // neighbours' (X, V): the committed position xo (w = p0.w), velocity vo
 // (w = v0.w) and, when vorticity is on, omega4 = (omega, |omega|).
-template <class Walk>
+template <class XS, class VS, class Walk>
 __device__ __forceinline__ void integrate_core(const DevParams& P, const float* bmin, const float* bmax,
-                                               const SdfDev& sdf, const float4* __restrict__ X,
-                                               const float4* __restrict__ V, float4 x4, float4 v0, float4 p0,
+                                               const SdfDev& sdf, XS X, VS V, float4 x4, float4 v0, float4 p0,
                                                Walk&& walk, float4& xo, float4& vo, float4& omega4)
 {
     float fx = 0.f, fy = 0.f, fz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
     if (P.visc_on || P.vort_on) {
         walk([&](float r2) { return r2 <= P.h2; },
              [&](int k) {
-                 const float4 xj = __ldg(X + k);
+                 const float4 xj = X[k];
                  const float rx = x4.x - xj.x, ry = x4.y - xj.y, rz = x4.z - xj.z;
                  const float r2 = rx * rx + ry * ry + rz * rz;
-                 const float4 vj = __ldg(V + k);
+                 const float4 vj = V[k];
                  const float ux = vj.x - v0.x, uy = vj.y - v0.y, uz = vj.z - v0.z;
                  if (P.visc_on) {
                      const float w = poly6_in(P, r2) * P.inv_rho0;
@@ -296,7 +314,8 @@ __device__ __forceinline__ void integrate_particle(const DevParams& P, const int
     const float4 v0 = __ldg(sv + s);
     const float4 p0 = sx0[s];
     float4 xo, vo, om;
-    integrate_core(P, bmin, bmax, sdf, xs, sv, x4, v0, p0, HashWalk{P, table, mask, xs, x4, s}, xo, vo, om);
+    integrate_core(P, bmin, bmax, sdf, GSrc{xs}, GSrc{sv}, x4, v0, p0, HashWalk{P, table, mask, xs, x4, s}, xo, vo,
+                   om);
     if (P.vort_on) somega[s] = om;
     const uint32_t id = __ldg(ids + s);
     pos[id] = xo;
@@ -307,18 +326,18 @@ __device__ __forceinline__ void integrate_particle(const DevParams& P, const int
 // ---- CS_VorticityConfinement.glsl:133-167 (pass 1) ----------------------------------------------
 // Velocity increment eps (N x omega_i) dt of a particle at xi with vorticity
 // w; returns false when |eta| < 1e-6 (no change).
-template <class Walk>
-__device__ __forceinline__ bool vorticity_core(const DevParams& P, const float4* __restrict__ X,
-                                               const float4* __restrict__ OM, float4 xi, float4 w, Walk&& walk,
+// MS: source of the neighbours' |omega| (MS[k] -> float).
+template <class XS, class MS, class Walk>
+__device__ __forceinline__ bool vorticity_core(const DevParams& P, XS X, MS OMAG, float4 xi, float4 w, Walk&& walk,
                                                float3& dv)
 {
     float ex = 0.f, ey = 0.f, ez = 0.f;
     walk([&](float r2) { return r2 <= P.h2 && r2 >= 1e-10f; },
          [&](int k) {
-             const float4 xj = __ldg(X + k);
+             const float4 xj = X[k];
              const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
              const float r2 = rx * rx + ry * ry + rz * rz;
-             const float sc = spiky_scale(P, r2) * __ldg(&OM[k].w);
+             const float sc = spiky_scale(P, r2) * OMAG[k];
              ex += rx * sc;
              ey += ry * sc;
              ez += rz * sc;
@@ -341,7 +360,8 @@ __device__ __forceinline__ void vorticity_particle(const DevParams& P, const int
 {
     const float4 xi = __ldg(spos + s);
     float3 dv;
-    if (!vorticity_core(P, spos, somega, xi, __ldg(somega + s), HashWalk{P, table, mask, spos, xi, s}, dv)) return;
+    if (!vorticity_core(P, GSrc{spos}, GMag{somega}, xi, __ldg(somega + s), HashWalk{P, table, mask, spos, xi, s}, dv))
+        return;
     const uint32_t id = __ldg(ids + s);
     float4 v = vel[id];
     v.x += dv.x;

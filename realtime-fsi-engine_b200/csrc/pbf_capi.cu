@@ -540,6 +540,8 @@ int pbf_handle::stage(int st, uint32_t iter)
             launch_lambda_m(P, sx[0], sx[1], rho, table, lod, iter, order, stream);
         else if (mode == 5)
             launch_lambda_s(P, sx[0], sx[1], rho, table, lod, iter, order, device, stream);
+        else if (mode == 7)
+            launch_lambda_b(P, sx[0], sx[1], rho, table, lod, iter, order, mcode, scalars + 3, stream);
         else
             launch_lambda(P, sx[0], sx[1], rho, table, lod, iter, order, stream);
         ++launches;
@@ -556,6 +558,8 @@ int pbf_handle::stage(int st, uint32_t iter)
             launch_deltap_m(P, sx[1], sx[0], table, lod, iter, order, stream);
         else if (mode == 5)
             launch_deltap_s(P, sx[1], sx[0], table, lod, iter, order, device, stream);
+        else if (mode == 7)
+            launch_deltap_b(P, sx[1], sx[0], table, lod, iter, order, mcode, scalars + 3, stream);
         else
             launch_deltap_apply(P, sx[1], sx[0], table, lod, iter, order, stream);
         ++launches;
@@ -573,6 +577,8 @@ int pbf_handle::stage(int st, uint32_t iter)
             launch_integrate_m(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, stream);
         else if (mode == 5)
             launch_integrate_s(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, device, stream);
+        else if (mode == 7)
+            launch_integrate_b(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, mcode, scalars + 3, stream);
         else
             launch_integrate(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, stream);
         ++launches;
@@ -588,6 +594,8 @@ int pbf_handle::stage(int st, uint32_t iter)
             launch_vorticity_m(P, sx0, somega, ids, vel, table, order, stream);
         else if (mode == 5)
             launch_vorticity_s(P, sx0, somega, ids, vel, table, order, device, stream);
+        else if (mode == 7)
+            launch_vorticity_b(P, sx0, somega, ids, vel, table, order, mcode, scalars + 3, stream);
         else
             launch_vorticity(P, sx0, somega, ids, vel, table, order, stream);
         ++launches;
@@ -679,6 +687,7 @@ extern "C" int pbf_create(const pbf_fluid_config* cfg, int device, pbf_handle** 
     for (int i = 0; i < PBF_NUM_PASS_SLOTS; ++i) h->prof_open[i] = -1;
     cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
     staged_init(device);
+    brick_init(device);
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         delete h;
@@ -1170,7 +1179,7 @@ extern "C" int pbf_set_option(pbf_handle* h, int option, int value)
     if (!h) return set_error(PBF_ERR_INVALID, "null handle");
     switch (option) {
     case PBF_OPT_SPATIAL_ORDER:
-        if (value < 0 || value > 6) return set_error(PBF_ERR_INVALID, "spatial order mode %d", value);
+        if (value < 0 || value > 7) return set_error(PBF_ERR_INVALID, "spatial order mode %d", value);
         h->pass_mode = value;
         h->label_space = false;
         break;
@@ -1189,6 +1198,18 @@ extern "C" int pbf_list_stats(pbf_handle* h, uint32_t* full_walks, uint32_t* buc
     CHECK_HANDLE(h);
     if (!full_walks || !bucket_walks || !marked_buckets) return set_error(PBF_ERR_INVALID, "null argument");
     *full_walks = *bucket_walks = *marked_buckets = 0;
+    if (h->effective_mode() == 7) {
+        // mode 7: blocks that walked global memory instead of their staged
+        // neighbourhood, counted since the handle was created
+        if (h->scalars) {
+            uint32_t d2[2];
+            CK(cudaMemcpyAsync(d2, h->scalars + 3, sizeof(d2), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            *full_walks = d2[0];    // blocks
+            *bucket_walks = d2[1];  // particles
+        }
+        return PBF_OK;
+    }
     if (!h->lstats) return PBF_OK;
     uint32_t d[4];
     CK(cudaMemcpyAsync(d, h->lstats, sizeof(d), cudaMemcpyDeviceToHost, h->stream));

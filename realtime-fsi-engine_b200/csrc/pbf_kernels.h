@@ -83,6 +83,22 @@ void launch_integrate_s(const DevParams& P, const float4* xs, const float4* sv, 
 void launch_vorticity_s(const DevParams& P, const float4* spos, const float4* somega, const uint32_t* ids,
                         float4* vel, const int2* table, const uint32_t* order, int device, cudaStream_t st);
 
+// ---- k_brick.cu: per-block neighbourhood staged in shared memory (dense cells) --
+// mcode: the reorder kernel's Morton code of each slot's predict-time cell;
+// stats (may be null): [0] blocks, [1] particles that walked global memory.
+void brick_init(int device);
+void launch_lambda_b(const DevParams& P, const float4* xin, float4* xout, float* rho, const int2* table,
+                     const uint32_t* lod, uint32_t iter, const uint32_t* order, const uint32_t* mcode,
+                     uint32_t* stats, cudaStream_t st);
+void launch_deltap_b(const DevParams& P, const float4* xin, float4* xout, const int2* table, const uint32_t* lod,
+                     uint32_t iter, const uint32_t* order, const uint32_t* mcode, uint32_t* stats, cudaStream_t st);
+void launch_integrate_b(const DevParams& P, const float4* xs, const float4* sv, float4* sx0, float4* somega,
+                        const uint32_t* ids, float4* pos, float4* vel, const int2* table, const uint32_t* order,
+                        const uint32_t* mcode, uint32_t* stats, cudaStream_t st);
+void launch_vorticity_b(const DevParams& P, const float4* spos, const float4* somega, const uint32_t* ids,
+                        float4* vel, const int2* table, const uint32_t* order, const uint32_t* mcode,
+                        uint32_t* stats, cudaStream_t st);
+
 // ---- k_list.cu: neighbour lists with a skin over Morton-labelled data ----------
 struct ListArgs {
     const int2* table;

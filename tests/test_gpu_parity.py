@@ -88,7 +88,8 @@ def test_cell_table_bit_exact(have_gpu):
                          [("glsl_stages_scorr.npz", 2), ("glsl_stages_apbf.npz", 2), ("glsl_stages_sdf.npz", 2),
                           ("glsl_stages_plain.npz", 0)] +
                          [(f, 3) for f in STAGE_FIXTURES] + [(f, 4) for f in STAGE_FIXTURES] +
-                         [(f, 5) for f in STAGE_FIXTURES] + [(f, 6) for f in STAGE_FIXTURES])
+                         [(f, 5) for f in STAGE_FIXTURES] + [(f, 6) for f in STAGE_FIXTURES] +
+                         [(f, 7) for f in STAGE_FIXTURES])
 def test_stages_match_oracle(have_gpu, name, mode):
     z = H.load(name)
     fl, sdf = make_fluid(z, mode)
@@ -308,14 +309,15 @@ def test_staged_blocks_fall_back_when_sparse(have_gpu):
     cfg.enable_scorr = 0
     cfg.particle_count = len(pos)
     outs = []
-    for mode in (4, 5):
+    for mode in (4, 5, 7):
         fl = P.PBFluids(cfg)
         fl.set_option(1, mode)
         fl.setParticles(P.make_particles(pos, vel))
         fl.step()
         outs.append(fl.readbackParticles())
-    assert np.abs(outs[0]["pos"] - outs[1]["pos"]).max() < 1e-5 * cfg.h
-    assert np.abs(outs[0]["vel"] - outs[1]["vel"]).max() < 1e-3
+    for o in outs[1:]:
+        assert np.abs(outs[0]["pos"] - o["pos"]).max() < 1e-5 * cfg.h
+        assert np.abs(outs[0]["vel"] - o["vel"]).max() < 1e-3
 
 
 def test_cooperative_and_per_thread_passes_agree(have_gpu):
@@ -325,7 +327,7 @@ def test_cooperative_and_per_thread_passes_agree(have_gpu):
     cfg, pos, vel = scenes.c0(16, seed=4)
     cfg.enable_scorr = 0
     outs = {}
-    for mode in (1, 0, 2, 2, 3, 3, 4, 5, 5, 6, 6):
+    for mode in (1, 0, 2, 2, 3, 3, 4, 5, 5, 6, 6, 7, 7):
         fl = P.PBFluids(cfg)
         fl.set_option(1, mode)
         fl.setParticles(P.make_particles(pos, vel))
@@ -335,7 +337,7 @@ def test_cooperative_and_per_thread_passes_agree(have_gpu):
             assert np.array_equal(outs[mode]["pos"], o["pos"]) and np.array_equal(outs[mode]["vel"], o["vel"])
         outs[mode] = o
     assert np.array_equal(outs[0]["pos"], outs[1]["pos"]) and np.array_equal(outs[0]["vel"], outs[1]["vel"])
-    for m in (2, 3, 4, 5, 6):
+    for m in (2, 3, 4, 5, 6, 7):
         assert np.abs(outs[m]["pos"] - outs[1]["pos"]).max() < 1e-5 * cfg.h
         assert np.abs(outs[m]["vel"] - outs[1]["vel"]).max() < 1e-3
 
