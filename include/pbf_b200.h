@@ -399,6 +399,45 @@ typedef struct pbf_batch_tuning {
 int pbf_batch_autotune(pbf_batch* b, uint32_t trial_steps, pbf_batch_tuning* best, pbf_batch_tuning* results,
                        uint32_t max_results, uint32_t* num_results);
 
+/* ---- host deformation (the consumer of pbf_vertex_forces) -------------------
+ * Cotangent-Laplacian surface deformation of a triangle mesh driven by
+ * per-vertex handle targets: LaplacianDeformation (include/deformation/
+ * LaplacianDeformation.h:11-157, src/deformation/LaplacianDeformation.cpp) and
+ * the application's per-frame handle logic deformStep (src/main.cpp:870-944),
+ * restated without Eigen/CHOLMOD/OpenMesh.  Host code, FP64 positions. */
+typedef struct pbf_deform pbf_deform;
+
+/* SceneDeform (include/core/Scene.h:17-27) / main.cpp's g_* tuning. */
+typedef struct pbf_deform_params {
+    float stiffness;             /* force -> displacement gain                  */
+    float max_displacement;      /* per-frame displacement clamp                */
+    float max_total_disp;        /* clamp on |deformed - rest|                  */
+    uint32_t restore_enabled;    /* elastic spring-back toward rest             */
+    float restore_strength;      /* fraction of the offset removed per frame    */
+    float control_threshold;     /* |force| to enter the handle set             */
+    float control_threshold_low; /* |force| to leave it (hysteresis)            */
+} pbf_deform_params;
+
+int pbf_deform_default_params(pbf_deform_params* out);
+/* verts3: nv x 3 rest positions; faces3: nf x 3 vertex indices. */
+int pbf_deform_create(const double* verts3, int32_t nv, const int32_t* faces3, int32_t nf, pbf_deform** out);
+int pbf_deform_destroy(pbf_deform* d);
+/* setUseLocal / setLocalKRing / setUseIncremental (defaults 1, 3, 0). */
+int pbf_deform_set_mode(pbf_deform* d, int32_t use_local, int32_t kring, int32_t use_incremental);
+int pbf_deform_add_anchor(pbf_deform* d, int32_t vertex);
+int pbf_deform_set_control_points(pbf_deform* d, const int32_t* indices, const double* targets3, int32_t n);
+int pbf_deform_precompute(pbf_deform* d);
+int pbf_deform_solve(pbf_deform* d);
+int pbf_deform_vertices(pbf_deform* d, double* out3, int32_t nv);
+int pbf_deform_set_vertices(pbf_deform* d, const double* verts3, int32_t nv);
+/* One frame: handle set from the forces (nv x 3), refactor when the set
+ * changed, solve; *moved = 1 when the mesh was re-solved. */
+int pbf_deform_step(pbf_deform* d, const float* forces3, int32_t nv, float dt, const pbf_deform_params* params,
+                    int32_t* handle_count, int32_t* refactored, int32_t* moved);
+int pbf_deform_patch_size(pbf_deform* d, int32_t* size);
+/* Incremental path: max |x - x_dense| on the x axis (-1 if not ready). */
+int pbf_deform_verify_incremental(pbf_deform* d, double* max_diff);
+
 /* ---- differentiable step ----------------------------------------------------
  * No reference counterpart.  Reverse-mode derivative of one step of a batch
  * (all substeps x iterations, then vorticity) with respect to the initial

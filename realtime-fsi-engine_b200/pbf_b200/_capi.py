@@ -89,6 +89,14 @@ class BatchTuning(C.Structure):
                 ("ms_per_step", C.c_float)]
 
 
+class DeformParams(C.Structure):
+    """pbf_deform_params == SceneDeform's handle policy (include/core/Scene.h:17-27)."""
+
+    _fields_ = [("stiffness", C.c_float), ("max_displacement", C.c_float), ("max_total_disp", C.c_float),
+                ("restore_enabled", C.c_uint32), ("restore_strength", C.c_float),
+                ("control_threshold", C.c_float), ("control_threshold_low", C.c_float)]
+
+
 BATCH_ALL = 0xFFFFFFFF
 BOPT_BLOCK, BOPT_ORDER, BOPT_BLOCKS_PER_SM, BOPT_USE_GRAPH = 1, 2, 3, 4
 
@@ -171,6 +179,20 @@ SIGNATURES = [
     ("pbf_batch_set_option", C.c_int, [vp, C.c_int, C.c_int]),
     ("pbf_batch_get_option", C.c_int, [vp, C.c_int, P(C.c_int)]),
     ("pbf_batch_autotune", C.c_int, [vp, u32, vp, vp, u32, P(u32)]),
+    # host deformation
+    ("pbf_deform_default_params", C.c_int, [P(DeformParams)]),
+    ("pbf_deform_create", C.c_int, [vp, i32, vp, i32, P(vp)]),
+    ("pbf_deform_destroy", C.c_int, [vp]),
+    ("pbf_deform_set_mode", C.c_int, [vp, i32, i32, i32]),
+    ("pbf_deform_add_anchor", C.c_int, [vp, i32]),
+    ("pbf_deform_set_control_points", C.c_int, [vp, vp, vp, i32]),
+    ("pbf_deform_precompute", C.c_int, [vp]),
+    ("pbf_deform_solve", C.c_int, [vp]),
+    ("pbf_deform_vertices", C.c_int, [vp, vp, i32]),
+    ("pbf_deform_set_vertices", C.c_int, [vp, vp, i32]),
+    ("pbf_deform_step", C.c_int, [vp, vp, i32, C.c_float, P(DeformParams), P(i32), P(i32), P(i32)]),
+    ("pbf_deform_patch_size", C.c_int, [vp, P(i32)]),
+    ("pbf_deform_verify_incremental", C.c_int, [vp, P(C.c_double)]),
     # differentiable step
     ("pbf_batch_set_sdf_offset", C.c_int, [vp, u32, P(C.c_float)]),
     ("pbf_batch_set_state", C.c_int, [vp, vp, vp]),
