@@ -49,10 +49,11 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", type=int, default=4, choices=[0, 1, 2, 3, 4, 5, 6, 7],
+    ap.add_argument("--mode", type=int, default=4, choices=[0, 1, 2, 3, 4, 5, 6, 7, 8],
                     help="neighbour passes: 0 hash order, 1 Morton, 2 Morton cell-cooperative, "
                          "3 Morton with per-lane pair queues, 4 Morton with per-bucket hit masks (default), "
-                         "5 Morton cell blocks staged through shared memory")
+                         "5 Morton cell blocks staged through shared memory, 6 neighbour lists with a skin, "
+                         "7 per-block dense cell box in shared memory, 8 x-runs of a dense cell window")
     ap.add_argument("--sample", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
                     help="smaller lattice of the same scene (profiling captures only)")
     return ap.parse_args()
@@ -258,6 +259,7 @@ def run_b200(args, dist):
     torch.cuda.synchronize(dev)
     clocks = Clocks(dev)
     l0 = fl.kernel_launches()
+    ws0 = fl.list_stats() if args.mode in (6, 7, 8) else None
     e0.record(stream)
     for _ in range(args.steps):
         fl.step()
@@ -267,6 +269,7 @@ def run_b200(args, dist):
     dist.barrier()
     clk = clocks.stop()
     launches = fl.kernel_launches() - l0
+    ws1 = fl.list_stats() if ws0 is not None else None
     ms = e0.elapsed_time(e1)
     passes = fl.pass_times()
     fl.set_profiling(False)
@@ -327,6 +330,9 @@ def run_b200(args, dist):
                        "l2": "working set >> 126 MB L2 (no flush needed)"},
             "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
             "passes": per_pass, "nonfinite_particles": int(bad), "impl": "b200"}
+    if ws1 is not None:
+        # pbf_list_stats before and after the timed steps (meaning per mode in pbf_b200.h)
+        line["walk_stats"] = {"before": list(ws0), "after": list(ws1)}
     if dist.rank == 0:
         print(json.dumps(line), flush=True)
     del obstacle

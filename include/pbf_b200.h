@@ -305,6 +305,14 @@ int pbf_set_use_graph(pbf_handle* h, int on);
  *                          7: Morton order, each 256-particle block stages the
  *                          buckets of its widened cell box in shared memory
  *                          (dense cell table) and walks them there.
+ *                          8: data relabelled by the slot of each particle's
+ *                          cell in a dense window of the box (z, y, x), so
+ *                          the three x-adjacent cells of a row are one label
+ *                          range: 9 runs replace the 27 buckets wherever the
+ *                          cell's neighbourhood has no hash collision and no
+ *                          particle within reach has moved 0.9 h since the
+ *                          predict; the hashed buckets elsewhere (APBF runs
+ *                          mode 4).
  *                          Every mode gives the same results up to FP32
  *                          contraction differences.
  *   PBF_OPT_LIST_SKIN      mode 6 list reach beyond h, in 1/1000 h (default 100). */
@@ -315,7 +323,12 @@ int pbf_set_option(pbf_handle* h, int option, int value);
 /* Mode 6 statistics of the last substep, summed over its passes: particles
  * that walked all 27 buckets instead of their list (moved more than skin/2
  * or changed cell), marked buckets walked in full from a list, and buckets
- * marked because one of their particles moved more than skin/2. */
+ * marked because one of their particles moved more than skin/2.
+ * Mode 7: blocks and particles that walked global memory (since creation).
+ * Mode 8: particle passes that walked the hashed buckets (since the window was
+ * set up), particles beyond the 0.9 h drift bound that marked the cells within
+ * their reach in the last substep (a same-bucket cell was near; counted per
+ * pass), and window cells whose neighbourhood has a hash collision. */
 int pbf_list_stats(pbf_handle* h, uint32_t* full_walks, uint32_t* bucket_walks, uint32_t* marked_buckets);
 
 /* ---- health ------------------------------------------------------------- */

@@ -1,0 +1,430 @@
+// k_dense.cu — neighbour mode 8: the hashed buckets replaced, where that is
+// exact, by runs of a dense cell window.
+//
+// The scene's box plus two cells on each side is a dense window of cells.
+// After the hash sort of a substep, every particle is relabelled by the
+// window slot of its predict-time cell (z, then y, then x; cells outside the
+// window wrap into it) and the per-particle arrays are gathered into that
+// label order.  The three x-adjacent cells of a row are then one contiguous
+// label range, so a particle walks 9 runs of about 24 candidates instead of
+// 27 buckets of about 8 (the reference, CS_ComputeLambdas.glsl:126-150).
+//
+// The run walk visits exactly the pairs of the bucket walk, in the same order,
+// when for the particle's cell c
+//   (a) c and its 26 neighbours lie inside the window (no wrap), and
+//   (b) no cell M within Chebyshev distance 2 of c shares a hash bucket with a
+//       neighbour cell N of c other than itself (M = N), and
+//   (c) no particle within reach of c has moved more than 0.9 h from its
+//       predict-time position while a cell sharing its predict-time cell's
+//       bucket lies near enough to matter (below).
+// Bucket hash(N) holds the particles of N and of every cell colliding with
+// it; the reference tests them all against r <= h.  A particle that moved at
+// most 0.9 h and whose predict-time cell is at Chebyshev distance >= 3 from c
+// is more than 2h - 0.9h from c's box, so out of range; by (b) no other
+// colliding cell is nearer.  So the in-range candidates of bucket hash(N) are
+// N's own, in id order (the stable sort), and the run walk sees N's particles
+// in the same order; particles of other cells wrapped into N's slot are far
+// and fail r <= h.  Within a run the cells come x - 1, x, x + 1, the
+// reference's innermost loop.
+//
+// (a) and (b) depend only on the window and the hash mask: one flag per slot,
+// computed when either changes, as is, per cell, the distance to the nearest
+// other cell of its bucket.  For (c), every pass that moves particles checks
+// each particle now more than 0.9 h from its predict-time position: unless
+// that distance shows no colliding cell can be in a query's neighbourhood
+// (settle_drift), it marks the window cells within 1.01 h of where the
+// particle is ("dirty" for the rest of the substep): only a query in such a
+// cell can have it in range.  A
+// particle whose cell fails (a), (b) or (c) walks the 27 hashed buckets
+// (through the hash-slot -> label map).  Both walks test candidates in chunks
+// into a hit mask exactly as the hashed-bucket passes do, so a pair's
+// arithmetic is the same in every walk.
+#include "masked_body.cuh"
+#include "pbf_kernels.h"
+
+namespace pbf {
+
+constexpr int kDThreads = 128;
+
+__device__ __forceinline__ uint32_t wrap_axis(int c, int g0, uint32_t n)
+{
+    const long long d = (long long)c - (long long)g0;
+    if (d >= 0 && d < (long long)n) return (uint32_t)d;
+    long long r = d % (long long)n;
+    if (r < 0) r += (long long)n;
+    return (uint32_t)r;
+}
+
+__device__ __forceinline__ uint32_t dense_key(const DenseArgs& D, int cx, int cy, int cz)
+{
+    return (wrap_axis(cz, D.gz0, D.nz) * D.ny + wrap_axis(cy, D.gy0, D.ny)) * D.nx + wrap_axis(cx, D.gx0, D.nx);
+}
+
+// Window slot of each hash-sorted particle's predict-time cell.
+__global__ void __launch_bounds__(256) k_d_keys(DevParams P, DenseArgs D, const float4* __restrict__ sx,
+                                                uint32_t* __restrict__ dkey)
+{
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < P.n; s += stride) {
+        const float4 x = __ldg(sx + s);
+        dkey[s] = dense_key(D, cell_coord(x.x, P.h), cell_coord(x.y, P.h), cell_coord(x.z, P.h));
+    }
+}
+
+// Conditions (a) and (b) per window slot.
+__global__ void __launch_bounds__(128) k_d_clean(DenseArgs D, uint32_t mask, uint8_t* __restrict__ clean,
+                                                 uint32_t* __restrict__ unclean)
+{
+    const uint32_t slots = D.nx * D.ny * D.nz;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += stride) {
+        const uint32_t lx = s % D.nx, ly = (s / D.nx) % D.ny, lz = s / (D.nx * D.ny);
+        uint8_t ok = 0;
+        if (lx >= 1 && lx + 1 < D.nx && ly >= 1 && ly + 1 < D.ny && lz >= 1 && lz + 1 < D.nz) {
+            const int cx = D.gx0 + (int)lx, cy = D.gy0 + (int)ly, cz = D.gz0 + (int)lz;
+            uint32_t hn[27];
+#pragma unroll
+            for (int u = 0; u < 27; ++u)
+                hn[u] = grid_hash(cx + u % 3 - 1, cy + (u / 3) % 3 - 1, cz + u / 9 - 1, mask);
+            bool good = true;
+#pragma unroll 1
+            for (int m = 0; m < 125; ++m) {
+                const int mx = m % 5 - 2, my = (m / 5) % 5 - 2, mz = m / 25 - 2;
+                const uint32_t hm = grid_hash(cx + mx, cy + my, cz + mz, mask);
+                const bool inner = mx >= -1 && mx <= 1 && my >= -1 && my <= 1 && mz >= -1 && mz <= 1;
+                const int self_u = inner ? (mz + 1) * 9 + (my + 1) * 3 + (mx + 1) : -1;
+#pragma unroll
+                for (int u = 0; u < 27; ++u) good &= !(hm == hn[u] && u != self_u);
+            }
+            ok = good ? 1 : 0;
+            if (!good) atomicAdd(unclean, 1u);
+        }
+        clean[s] = ok;
+    }
+}
+
+// Chebyshev distance from each window cell to the nearest other cell in the
+// same hash bucket, searched up to kDcolReach (kDcolReach + 1: none that near).
+constexpr int kDcolReach = 6;
+__global__ void __launch_bounds__(128) k_d_dcol(DenseArgs D, uint32_t mask, uint8_t* __restrict__ dcol)
+{
+    const uint32_t slots = D.nx * D.ny * D.nz;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += stride) {
+        const int cx = D.gx0 + (int)(s % D.nx), cy = D.gy0 + (int)((s / D.nx) % D.ny), cz = D.gz0 + (int)(s / (D.nx * D.ny));
+        const uint32_t h0 = grid_hash(cx, cy, cz, mask);
+        int best = kDcolReach + 1;
+#pragma unroll 1
+        for (int mz = -kDcolReach; mz <= kDcolReach; ++mz) {
+#pragma unroll 1
+            for (int my = -kDcolReach; my <= kDcolReach; ++my) {
+                const uint32_t hyz = ((uint32_t)(cy + my) * kP2) ^ ((uint32_t)(cz + mz) * kP3);
+                const int dyz = max(abs(my), abs(mz));
+#pragma unroll 13
+                for (int mx = -kDcolReach; mx <= kDcolReach; ++mx) {
+                    const bool hit = ((((uint32_t)(cx + mx) * kP1) ^ hyz) & mask) == h0 && (mx | my | mz) != 0;
+                    if (hit) best = min(best, max(dyz, abs(mx)));
+                }
+            }
+        }
+        dcol[s] = (uint8_t)best;
+    }
+}
+
+// Candidates lo .. hi-1 of one run in chunks of kChunk, tested into a hit
+// mask; the body runs for the hits in candidate order (masked_walk's scheme).
+// map(k) gives the label of candidate k (identity for a run; the hash-slot
+// -> label map for a bucket).
+template <class Map, class Hit, class Body>
+__device__ __forceinline__ void masked_range(const float4* __restrict__ X, float4 xi, int self, int lo, int hi,
+                                             Map&& map, Hit&& hit, Body&& body)
+{
+#pragma unroll 1
+    for (int k0 = lo; k0 < hi; k0 += kChunk) {
+        uint32_t m = 0;
+#pragma unroll
+        for (int c = 0; c < kChunk; ++c) {
+            const int k = k0 + c;
+            if (k < hi) {
+                const int j = map(k);
+                const float4 xj = __ldg(X + j);
+                const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+                if (hit(rx * rx + ry * ry + rz * rz) && j != self) m |= 1u << c;
+            }
+        }
+        while (m) {
+            const int c = __ffs(m) - 1;
+            m &= m - 1u;
+            body(map(k0 + c));
+        }
+    }
+}
+
+struct IdMap {
+    __device__ __forceinline__ int operator()(int k) const { return k; }
+};
+struct InvMap {
+    const uint32_t* __restrict__ inv;
+    __device__ __forceinline__ int operator()(int k) const { return (int)__ldg(inv + k); }
+};
+
+// The 9 x-runs of a particle whose cell satisfies (a), (b) and (c).
+struct RunWalk {
+    const int2* __restrict__ table;
+    const float4* __restrict__ X;
+    float4 xi;
+    int self;
+    int s0;  // window slot of the particle's cell
+    int nx, nxy;
+    template <class Hit, class Body>
+    __device__ __forceinline__ void operator()(Hit&& hit, Body&& body) const
+    {
+#pragma unroll 1
+        for (int dz = -1; dz <= 1; ++dz) {
+#pragma unroll 1
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int s = s0 + dz * nxy + dy * nx;
+                const int2 e0 = __ldg(table + s - 1), e1 = __ldg(table + s), e2 = __ldg(table + s + 1);
+                const int hi = max(max(e0.y, e1.y), e2.y);
+                if (hi < 0) continue;
+                // empty slots hold (-1, -1): as unsigned their start is the largest
+                const int lo = (int)min(min((uint32_t)e0.x, (uint32_t)e1.x), (uint32_t)e2.x);
+                masked_range(X, xi, self, lo, hi, IdMap{}, hit, body);
+            }
+        }
+    }
+};
+
+// The 27 hashed buckets in label space, in the reference's order.
+struct BucketWalkLabels {
+    const DevParams& P;
+    const int2* __restrict__ htable;
+    const uint32_t* __restrict__ inv;
+    const float4* __restrict__ X;
+    float4 xi;
+    int self;
+    template <class Hit, class Body>
+    __device__ __forceinline__ void operator()(Hit&& hit, Body&& body) const
+    {
+        const int cx = cell_coord(xi.x, P.h), cy = cell_coord(xi.y, P.h), cz = cell_coord(xi.z, P.h);
+#pragma unroll 1
+        for (int dz = -1; dz <= 1; ++dz) {
+            const uint32_t hz = (uint32_t)(cz + dz) * kP3;
+#pragma unroll 1
+            for (int dy = -1; dy <= 1; ++dy) {
+                const uint32_t hyz = hz ^ ((uint32_t)(cy + dy) * kP2);
+#pragma unroll 1
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int2 se = __ldg(htable + ((((uint32_t)(cx + dx) * kP1) ^ hyz) & P.mask));
+                    if (se.x == -1) continue;
+                    masked_range(X, xi, self, se.x, se.y, InvMap{inv}, hit, body);
+                }
+            }
+        }
+    }
+};
+
+// Run core(walker) with the run walk when (a), (b) and (c) hold, else with
+// the bucket walk.
+template <class Core>
+__device__ __forceinline__ void with_dense_walker(const DevParams& P, const DenseArgs& D, const float4* X, float4 xi,
+                                                  int t, Core&& core)
+{
+    const uint32_t ux = (uint32_t)cell_coord(xi.x, P.h) - (uint32_t)D.gx0;
+    const uint32_t uy = (uint32_t)cell_coord(xi.y, P.h) - (uint32_t)D.gy0;
+    const uint32_t uz = (uint32_t)cell_coord(xi.z, P.h) - (uint32_t)D.gz0;
+    if (ux - 1u < D.nx - 2u && uy - 1u < D.ny - 2u && uz - 1u < D.nz - 2u) {
+        const int s0 = (int)((uz * D.ny + uy) * D.nx + ux);
+        if (__ldg(D.clean + s0) && !D.dirty[s0]) {
+            core(RunWalk{D.table, X, xi, t, s0, (int)D.nx, (int)(D.nx * D.ny)});
+            return;
+        }
+    }
+    const uint32_t am = __activemask();
+    if ((threadIdx.x & 31u) == (uint32_t)(__ffs(am) - 1)) atomicAdd(D.flag + 1, (uint32_t)__popc(am));
+    core(BucketWalkLabels{P, D.htable, D.inv, X, xi, t});
+}
+
+// A particle at x, predict-time position xb, that has moved more than the
+// 0.9 h bound.  It can differ between the two walks only for a query whose
+// neighbour cells include a cell N != M (M = its predict-time cell) with
+// hash(N) = hash(M), and only if the query is within reach of x.  Such
+// queries lie within Chebyshev distance 2 of x's cell (1.01 h reach), their
+// neighbour cells within 3, so within 3 + cheb(cell(x), M) of M.  When M's
+// nearest same-bucket cell is farther (dcol), the particle is harmless;
+// otherwise the cells within reach of x are marked dirty.  Kept out of line:
+// it takes no registers from the passes.
+__device__ __noinline__ void settle_drift(const uint8_t* dcol, uint8_t* dirty, uint32_t* count, float h, float x,
+                                          float y, float z, float bx, float by, float bz, int gx0, int gy0, int gz0,
+                                          uint32_t nx, uint32_t ny, uint32_t nz)
+{
+    const float c[3] = {x, y, z}, cb[3] = {bx, by, bz};
+    const int g0[3] = {gx0, gy0, gz0};
+    const uint32_t nd[3] = {nx, ny, nz};
+    long long cheb = 0;
+    uint32_t um[3];
+    bool inside = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int m = cell_coord(cb[a], h);
+        const long long d = (long long)cell_coord(c[a], h) - (long long)m;
+        cheb = max(cheb, d < 0 ? -d : d);
+        um[a] = (uint32_t)m - (uint32_t)g0[a];
+        inside = inside && um[a] < nd[a];
+    }
+    if (inside && cheb + 3 < (long long)dcol[(um[2] * ny + um[1]) * nx + um[0]]) return;
+    atomicAdd(count, 1u);
+    const float r = 1.01f * h;
+    uint32_t lo[3];
+    int cnt[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int l = cell_coord(c[a] - r, h), hgh = cell_coord(c[a] + r, h);
+        const long long d = (long long)hgh - (long long)l;
+        cnt[a] = d < 0 ? 0 : (d > 3 ? 4 : (int)d + 1);
+        lo[a] = (uint32_t)l - (uint32_t)g0[a];
+    }
+    for (int iz = 0; iz < cnt[2]; ++iz) {
+        const uint32_t uz = lo[2] + (uint32_t)iz;
+        if (uz >= nz) continue;
+        for (int iy = 0; iy < cnt[1]; ++iy) {
+            const uint32_t uy = lo[1] + (uint32_t)iy;
+            if (uy >= ny) continue;
+            for (int ix = 0; ix < cnt[0]; ++ix) {
+                const uint32_t ux = lo[0] + (uint32_t)ix;
+                if (ux < nx) dirty[(uz * ny + uy) * nx + ux] = 1;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void check_drift(const DevParams& P, const DenseArgs& D, float4 x, int t)
+{
+    const float4 b = __ldg(D.xb + t);
+    const float dx = x.x - b.x, dy = x.y - b.y, dz = x.z - b.z;
+    // NaN positions count as moved (the comparison is false for NaN)
+    if (!(dx * dx + dy * dy + dz * dz <= D.drift2))
+        settle_drift(D.dcol, D.dirty, D.flag, P.h, x.x, x.y, x.z, b.x, b.y, b.z, D.gx0, D.gy0, D.gz0, D.nx, D.ny,
+                     D.nz);
+}
+
+__global__ void __launch_bounds__(kDThreads) k_d_lambda(DevParams P, DenseArgs D, const float4* __restrict__ lx_in,
+                                                        float4* __restrict__ lx_out, float* __restrict__ lrho)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int)P.n) return;
+    const float4 xi = __ldg(lx_in + t);
+    float rho, den;
+    float3 g;
+    float4 out;
+    with_dense_walker(P, D, lx_in, xi, t,
+                      [&](auto&& walk) { out = lambda_core(P, GSrc{lx_in}, xi, walk, rho, g, den); });
+    lx_out[t] = out;
+    lrho[t] = rho;
+}
+
+__global__ void __launch_bounds__(kDThreads) k_d_deltap(DevParams P, DenseArgs D, const float4* __restrict__ lx_in,
+                                                        float4* __restrict__ lx_out)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int)P.n) return;
+    const float4 xi = __ldg(lx_in + t);
+    float3 dp;
+    float4 out;
+    with_dense_walker(P, D, lx_in, xi, t,
+                      [&](auto&& walk) { out = deltap_core(P, P.sdf, GSrc{lx_in}, xi, walk, dp); });
+    lx_out[t] = out;
+    check_drift(P, D, out, t);
+}
+
+__global__ void __launch_bounds__(kDThreads) k_d_integrate(DevParams P, DenseArgs D, const float4* __restrict__ lx,
+                                                           const float4* __restrict__ lv, float4* __restrict__ lx0,
+                                                           float4* __restrict__ lom,
+                                                           const uint32_t* __restrict__ lid, float4* __restrict__ pos,
+                                                           float4* __restrict__ vel)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int)P.n) return;
+    const float4 x4 = __ldg(lx + t);
+    const float4 v0 = __ldg(lv + t);
+    const float4 p0 = lx0[t];
+    float4 xo, vo, om;
+    with_dense_walker(P, D, lx, x4, t, [&](auto&& walk) {
+        integrate_core(P, P.bmin, P.bmax, P.sdf, GSrc{lx}, GSrc{lv}, x4, v0, p0, walk, xo, vo, om);
+    });
+    if (P.vort_on) lom[t] = om;
+    const uint32_t id = __ldg(lid + t);
+    pos[id] = xo;
+    vel[id] = vo;
+    lx0[t] = xo;
+    check_drift(P, D, xo, t);
+}
+
+__global__ void __launch_bounds__(kDThreads) k_d_vorticity(DevParams P, DenseArgs D, const float4* __restrict__ lx0,
+                                                           const float4* __restrict__ lom,
+                                                           const uint32_t* __restrict__ lid, float4* __restrict__ vel)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int)P.n) return;
+    const float4 xi = __ldg(lx0 + t);
+    float3 dv;
+    bool any = false;
+    with_dense_walker(P, D, lx0, xi, t, [&](auto&& walk) {
+        any = vorticity_core(P, GSrc{lx0}, GMag{lom}, xi, __ldg(lom + t), walk, dv);
+    });
+    if (!any) return;
+    const uint32_t id = __ldg(lid + t);
+    float4 v = vel[id];
+    v.x += dv.x;
+    v.y += dv.y;
+    v.z += dv.z;
+    vel[id] = v;
+}
+
+// ---- launchers ------------------------------------------------------------------------------
+static inline unsigned dgrid(uint32_t n) { return (n + kDThreads - 1) / kDThreads; }
+static inline unsigned capped_grid(uint32_t n, uint32_t threads, int sms, uint32_t per_sm)
+{
+    const uint32_t want = (n + threads - 1u) / threads, cap = (uint32_t)sms * per_sm;
+    return want < 1 ? 1 : (want > cap ? cap : want);
+}
+
+void launch_d_keys(const DevParams& P, const DenseArgs& D, const float4* sx, uint32_t* dkey, int sms, cudaStream_t st)
+{
+    k_d_keys<<<capped_grid(P.n, 256, sms, 8), 256, 0, st>>>(P, D, sx, dkey);
+}
+
+void launch_d_clean(const DenseArgs& D, uint32_t mask, uint8_t* clean, uint32_t* unclean, int sms, cudaStream_t st)
+{
+    k_d_clean<<<capped_grid(D.nx * D.ny * D.nz, 128, sms, 16), 128, 0, st>>>(D, mask, clean, unclean);
+}
+
+void launch_d_dcol(const DenseArgs& D, uint32_t mask, uint8_t* dcol, int sms, cudaStream_t st)
+{
+    k_d_dcol<<<capped_grid(D.nx * D.ny * D.nz, 128, sms, 16), 128, 0, st>>>(D, mask, dcol);
+}
+
+void launch_d_lambda(const DevParams& P, const DenseArgs& D, const float4* lx_in, float4* lx_out, float* lrho,
+                     cudaStream_t st)
+{
+    k_d_lambda<<<dgrid(P.n), kDThreads, 0, st>>>(P, D, lx_in, lx_out, lrho);
+}
+
+void launch_d_deltap(const DevParams& P, const DenseArgs& D, const float4* lx_in, float4* lx_out, cudaStream_t st)
+{
+    k_d_deltap<<<dgrid(P.n), kDThreads, 0, st>>>(P, D, lx_in, lx_out);
+}
+
+void launch_d_integrate(const DevParams& P, const DenseArgs& D, const float4* lx, const float4* lv, float4* lx0,
+                        float4* lom, const uint32_t* lid, float4* pos, float4* vel, cudaStream_t st)
+{
+    k_d_integrate<<<dgrid(P.n), kDThreads, 0, st>>>(P, D, lx, lv, lx0, lom, lid, pos, vel);
+}
+
+void launch_d_vorticity(const DevParams& P, const DenseArgs& D, const float4* lx0, const float4* lom,
+                        const uint32_t* lid, float4* vel, cudaStream_t st)
+{
+    k_d_vorticity<<<dgrid(P.n), kDThreads, 0, st>>>(P, D, lx0, lom, lid, vel);
+}
+
+}  // namespace pbf

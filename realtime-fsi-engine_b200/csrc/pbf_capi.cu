@@ -317,6 +317,7 @@ pbf_handle::~pbf_handle()
     dfree(hist); dfree(totals); dfree(table); dfree(cand); dfree(ct_counts); dfree(scalars);
     dfree(lx[0]); dfree(lx[1]); dfree(lxb); dfree(lv); dfree(lx0); dfree(lom); dfree(lrho);
     dfree(lid); dfree(lkey); dfree(inv); dfree(list); dfree(lcnt); dfree(lstats); dfree(fastb);
+    dfree(dtable); dfree(dclean); dfree(ddcol); dfree(ddirty); dfree(dflag);
     dfree(grid); dfree(slab_min);
     mesh_free();
     if (stream) cudaStreamDestroy(stream);
@@ -377,22 +378,117 @@ int pbf_handle::prof_collect()
 // ---- neighbour lists (mode 6) ---------------------------------------------------------
 // Mode 6 needs every iteration to run (no APBF skips) and one displacement
 // slot per moving pass; otherwise the handle runs mode 4.
+// Mode 8 likewise (label arrays without APBF's per-particle skips), and only
+// when the dense window of the box stays within 2^26 cells.
 int pbf_handle::effective_mode() const
 {
-    if (pass_mode == 6 && (derived.enable_apbf || n >= (1u << 27))) return 4;
+    if ((pass_mode == 6 || pass_mode == 8) && (derived.enable_apbf || n >= (1u << 27))) return 4;
+    if (pass_mode == 8) {
+        int g0[3];
+        uint32_t nd[3];
+        if (!dense_window(g0, nd)) return 4;
+    }
     return pass_mode;
+}
+
+int pbf_handle::ensure_label_capacity()
+{
+    int rc;
+    if (cap_label_n < n || !inv) {
+        const size_t c = std::max<uint32_t>(n, 1u);
+        if ((rc = dalloc(lx[0], c)) || (rc = dalloc(lx[1], c)) || (rc = dalloc(lxb, c)) || (rc = dalloc(lv, c)) ||
+            (rc = dalloc(lx0, c)) || (rc = dalloc(lom, c)) || (rc = dalloc(lrho, c)) || (rc = dalloc(lid, c)) ||
+            (rc = dalloc(lkey, c)) || (rc = dalloc(inv, c)))
+            return rc;
+        cap_label_n = (uint32_t)c;
+    }
+    return PBF_OK;
+}
+
+// ---- dense cell window (mode 8) -----------------------------------------------------------
+// The walls' box in cells (floor(x / h) in FP32, as the kernels compute a
+// cell) with two cells of margin on each side.  Any window is correct (cells
+// outside wrap into it and their queries walk the hashed buckets); this one
+// puts every particle held by the walls in an interior cell.
+bool pbf_handle::dense_window(int g0[3], uint32_t nd[3]) const
+{
+    const float h = derived.h;
+    if (!(h > 0.0f)) return false;
+    uint64_t slots = 1;
+    for (int a = 0; a < 3; ++a) {
+        const float lo = std::floor(derived.bounds_min[a] / h), hi = std::floor(derived.bounds_max[a] / h);
+        if (!(lo >= -1e8f && hi <= 1e8f && hi >= lo)) return false;
+        g0[a] = (int)lo - 2;
+        nd[a] = (uint32_t)((int)hi - (int)lo + 5);
+        slots *= nd[a];
+    }
+    return slots <= (1ull << 26);
+}
+
+DenseArgs pbf_handle::dense_args() const
+{
+    DenseArgs D;
+    D.table = dtable;
+    D.clean = dclean;
+    D.dcol = ddcol;
+    D.dirty = ddirty;
+    D.htable = table;
+    D.inv = inv;
+    D.xb = lxb;
+    D.flag = dflag;
+    D.gx0 = dwin_g0[0];
+    D.gy0 = dwin_g0[1];
+    D.gz0 = dwin_g0[2];
+    D.nx = dwin_n[0];
+    D.ny = dwin_n[1];
+    D.nz = dwin_n[2];
+    const float b = 0.9f * derived.h;
+    D.drift2 = b * b;
+    return D;
+}
+
+// Buffers of mode 8 and the per-slot flags of the current window and hash
+// mask; recomputed (one kernel, then a synchronize) when either changes.  Runs
+// before any graph capture of the step.
+int pbf_handle::ensure_dense()
+{
+    int rc;
+    if ((rc = ensure_label_capacity())) return rc;
+    int g0[3];
+    uint32_t nd[3];
+    if (!dense_window(g0, nd)) return set_error(PBF_ERR_INVALID, "dense cell window larger than 2^26 cells");
+    const size_t slots = (size_t)nd[0] * nd[1] * nd[2];
+    const bool same = dwin_ready && dwin_mask == derived.hash_size - 1 && std::equal(g0, g0 + 3, dwin_g0) &&
+                      std::equal(nd, nd + 3, dwin_n);
+    if (same) return PBF_OK;
+    if (capturing) return set_error(PBF_ERR_INVALID, "dense cell window changed during graph capture");
+    if (slots > cap_slots || !dtable) {
+        if ((rc = dalloc(dtable, slots)) || (rc = dalloc(dclean, slots)) || (rc = dalloc(ddcol, slots)) ||
+            (rc = dalloc(ddirty, slots)))
+            return rc;
+        cap_slots = slots;
+    }
+    if (!dflag && (rc = dalloc(dflag, 4))) return rc;
+    std::copy(g0, g0 + 3, dwin_g0);
+    std::copy(nd, nd + 3, dwin_n);
+    dwin_mask = derived.hash_size - 1;
+    CK(cudaMemsetAsync(dflag, 0, 4 * sizeof(uint32_t), stream));
+    launch_d_clean(dense_args(), dwin_mask, dclean, dflag + 2, num_sms, stream);
+    launch_d_dcol(dense_args(), dwin_mask, ddcol, num_sms, stream);
+    launches += 2;
+    CK(cudaMemcpyAsync(&dwin_unclean, dflag + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    dwin_ready = true;
+    return PBF_OK;
 }
 
 int pbf_handle::ensure_list_capacity()
 {
     int rc;
+    if ((rc = ensure_label_capacity())) return rc;
     if (cap_list_n < n || !list) {
         const size_t c = std::max<uint32_t>(n, 1u);
-        if ((rc = dalloc(lx[0], c)) || (rc = dalloc(lx[1], c)) || (rc = dalloc(lxb, c)) || (rc = dalloc(lv, c)) ||
-            (rc = dalloc(lx0, c)) || (rc = dalloc(lom, c)) || (rc = dalloc(lrho, c)) || (rc = dalloc(lid, c)) ||
-            (rc = dalloc(lkey, c)) || (rc = dalloc(inv, c)) || (rc = dalloc(list, c * list_cap)) ||
-            (rc = dalloc(lcnt, c)) || (rc = dalloc(lstats, 4)))
-            return rc;
+        if ((rc = dalloc(list, c * list_cap)) || (rc = dalloc(lcnt, c)) || (rc = dalloc(lstats, 4))) return rc;
         cap_list_n = (uint32_t)c;
     }
     if (cap_fast != derived.hash_size || !fastb) {
@@ -485,6 +581,30 @@ int pbf_handle::stage(int st, uint32_t iter)
             break;  // predict, sort, table, reorder: below
         }
     }
+    if (mode == 8 && st >= PBF_STAGE_LAMBDA && st <= PBF_STAGE_VORTICITY) {
+        if (!label_space || !dwin_ready) return set_error(PBF_ERR_INVALID, "mode 8: run the reorder stage first");
+        const DenseArgs D = dense_args();
+        prof_begin(st);
+        switch (st) {
+        case PBF_STAGE_LAMBDA:
+            launch_d_lambda(P, D, lx[0], lx[1], lrho, stream);
+            last_x = 1;
+            break;
+        case PBF_STAGE_DELTAP:
+            launch_d_deltap(P, D, lx[1], lx[0], stream);
+            last_x = 0;
+            break;
+        case PBF_STAGE_INTEGRATE:
+            launch_d_integrate(P, D, lx[0], lv, lx0, lom, lid, pos, vel, stream);
+            break;
+        default:
+            launch_d_vorticity(P, D, lx0, lom, lid, vel, stream);
+            break;
+        }
+        ++launches;
+        prof_end(st);
+        return PBF_OK;
+    }
     switch (st) {
     case PBF_STAGE_PREDICT:
         prof_begin(PBF_STAGE_PREDICT);
@@ -509,9 +629,33 @@ int pbf_handle::stage(int st, uint32_t iter)
         break;
     case PBF_STAGE_REORDER:
         prof_begin(PBF_STAGE_REORDER);
-        launch_reorder(P, ids, pos, vel, sx[0], sv, sx0, lod, mode ? mcode : nullptr, sms, stream);
+        launch_reorder(P, ids, pos, vel, sx[0], sv, sx0, lod, mode && mode != 8 ? mcode : nullptr, sms, stream);
         ++launches;
         order = nullptr;
+        if (mode == 8) {
+            // relabel by window slot, then the slot table of the labels
+            int rc = ensure_dense();
+            if (rc) return rc;
+            const DenseArgs D = dense_args();
+            launch_d_keys(P, D, sx[0], mcode, sms, stream);
+            ++launches;
+            const uint64_t slots = (uint64_t)dwin_n[0] * dwin_n[1] * dwin_n[2];
+            uint32_t bits = 1;
+            while ((1ull << bits) < slots) ++bits;
+            uint32_t* msorted = nullptr;
+            launch_radix_sort(n, bits, mcode, mka, mia, mkb, mib, hist, totals, &msorted, &order, stream, &launches);
+            launch_l_permute(n, order, ids, skeys, sx[0], sv, sx0, lx[0], lxb, lv, lx0, lid, lkey, inv, sms, stream);
+            ++launches;
+            CK(cudaMemsetAsync(dtable, 0xFF, sizeof(int2) * slots, stream));
+            launch_build_table(n, msorted, dtable, sms, stream);
+            ++launches;
+            CK(cudaMemsetAsync(ddirty, 0, slots, stream));
+            CK(cudaMemsetAsync(dflag, 0, sizeof(uint32_t), stream));
+            label_space = true;
+            last_x = 0;
+            prof_end(PBF_STAGE_REORDER);
+            break;
+        }
         if (mode) {
             uint32_t* msorted = nullptr;
             launch_radix_sort(n, 24, mcode, mka, mia, mkb, mib, hist, totals, &msorted, &order, stream, &launches);
@@ -628,6 +772,10 @@ int pbf_handle::step()
     if (n == 0) return PBF_OK;  // PBFluids.cpp:325
     if (effective_mode() == 6) {
         const int rc = ensure_list_capacity();  // before any capture
+        if (rc) return rc;
+    }
+    if (effective_mode() == 8) {
+        const int rc = ensure_dense();  // allocation and slot flags before any capture
         if (rc) return rc;
     }
     const uint64_t gen = sdf_src ? sdf_src->grid_generation : 0;
@@ -1179,7 +1327,7 @@ extern "C" int pbf_set_option(pbf_handle* h, int option, int value)
     if (!h) return set_error(PBF_ERR_INVALID, "null handle");
     switch (option) {
     case PBF_OPT_SPATIAL_ORDER:
-        if (value < 0 || value > 7) return set_error(PBF_ERR_INVALID, "spatial order mode %d", value);
+        if (value < 0 || value > 8) return set_error(PBF_ERR_INVALID, "spatial order mode %d", value);
         h->pass_mode = value;
         h->label_space = false;
         break;
@@ -1198,6 +1346,21 @@ extern "C" int pbf_list_stats(pbf_handle* h, uint32_t* full_walks, uint32_t* buc
     CHECK_HANDLE(h);
     if (!full_walks || !bucket_walks || !marked_buckets) return set_error(PBF_ERR_INVALID, "null argument");
     *full_walks = *bucket_walks = *marked_buckets = 0;
+    if (h->effective_mode() == 8) {
+        // mode 8: particle passes that walked the hashed buckets since the
+        // window was set up, particles of the last substep that moved beyond
+        // the drift bound near a colliding cell and marked cells (counted per
+        // pass), window cells that fail the collision test
+        if (h->dflag) {
+            uint32_t d3[3];
+            CK(cudaMemcpyAsync(d3, h->dflag, sizeof(d3), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            *full_walks = d3[1];
+            *bucket_walks = d3[0];
+            *marked_buckets = d3[2];
+        }
+        return PBF_OK;
+    }
     if (h->effective_mode() == 7) {
         // mode 7: blocks that walked global memory instead of their staged
         // neighbourhood, counted since the handle was created

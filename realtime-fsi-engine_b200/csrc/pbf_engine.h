@@ -60,7 +60,24 @@ struct pbf_handle {
     uint32_t list_cap = 64;      // entries per particle
     float list_skin = 0.1f;      // in units of h
     bool label_space = false;    // the current substep's state lives in the label arrays
+    uint32_t cap_label_n = 0;
+    // mode 8: runs of a dense cell window (label arrays shared with mode 6)
+    int2* dtable = nullptr;      // per window slot: label range
+    uint8_t* dclean = nullptr;   // per window slot: no hash collision near the cell
+    uint8_t* ddcol = nullptr;    // per window slot: distance to the nearest other cell of its bucket
+    uint8_t* ddirty = nullptr;   // per window slot: a moved particle within reach (per substep)
+    uint32_t* dflag = nullptr;   // [0] drift-bound crossings, [1] bucket walks, [2] unclean slots
+    size_t cap_slots = 0;
+    int dwin_g0[3] = {0, 0, 0};
+    uint32_t dwin_n[3] = {0, 0, 0};
+    uint32_t dwin_mask = 0;
+    bool dwin_ready = false;
+    uint32_t dwin_unclean = 0;
+    bool dense_window(int g0[3], uint32_t nd[3]) const;
+    int ensure_dense();
+    pbf::DenseArgs dense_args() const;
     int effective_mode() const;
+    int ensure_label_capacity();
     int ensure_list_capacity();
     pbf::ListArgs list_args() const;
     int unpermute_for_read(int which);

@@ -127,6 +127,31 @@ void launch_l_vorticity(const DevParams& P, const ListArgs& A, const float4* lx0
 void launch_l_unpermute4(uint32_t n, const uint32_t* inv, const float4* src, float4* dst, int sms, cudaStream_t st);
 void launch_l_unpermute1(uint32_t n, const uint32_t* inv, const float* src, float* dst, int sms, cudaStream_t st);
 
+// ---- k_dense.cu: x-runs of a dense cell window over relabelled data ----------
+struct DenseArgs {
+    const int2* table;     // per window slot: label range of its particles, (-1, -1) when empty
+    const uint8_t* clean;  // per window slot: 1 = no hash collision near the cell
+    const uint8_t* dcol;   // per window slot: Chebyshev distance to the nearest other cell of its bucket
+    uint8_t* dirty;        // per window slot: a moved particle with a colliding cell near is within reach
+    const int2* htable;    // the hashed cell table (sorted slots)
+    const uint32_t* inv;   // hash slot -> label
+    const float4* xb;      // predict-time x*, label order
+    uint32_t* flag;        // [0] moved particles that marked cells this substep, [1] bucket walks
+    int gx0, gy0, gz0;     // cell coordinates of window slot (0, 0, 0)
+    uint32_t nx, ny, nz;   // window extent in cells
+    float drift2;          // squared drift bound (0.9 h)^2
+};
+void launch_d_keys(const DevParams& P, const DenseArgs& D, const float4* sx, uint32_t* dkey, int sms, cudaStream_t st);
+void launch_d_clean(const DenseArgs& D, uint32_t mask, uint8_t* clean, uint32_t* unclean, int sms, cudaStream_t st);
+void launch_d_dcol(const DenseArgs& D, uint32_t mask, uint8_t* dcol, int sms, cudaStream_t st);
+void launch_d_lambda(const DevParams& P, const DenseArgs& D, const float4* lx_in, float4* lx_out, float* lrho,
+                     cudaStream_t st);
+void launch_d_deltap(const DevParams& P, const DenseArgs& D, const float4* lx_in, float4* lx_out, cudaStream_t st);
+void launch_d_integrate(const DevParams& P, const DenseArgs& D, const float4* lx, const float4* lv, float4* lx0,
+                        float4* lom, const uint32_t* lid, float4* pos, float4* vel, cudaStream_t st);
+void launch_d_vorticity(const DevParams& P, const DenseArgs& D, const float4* lx0, const float4* lom,
+                        const uint32_t* lid, float4* vel, cudaStream_t st);
+
 // ---- k_sort.cu ----------------------------------------------------------------
 uint32_t sort_num_tiles(uint32_t n);
 void launch_radix_sort(uint32_t n, uint32_t key_bits, const uint32_t* keys_in, uint32_t* ka, uint32_t* ia,

@@ -89,7 +89,7 @@ def test_cell_table_bit_exact(have_gpu):
                           ("glsl_stages_plain.npz", 0)] +
                          [(f, 3) for f in STAGE_FIXTURES] + [(f, 4) for f in STAGE_FIXTURES] +
                          [(f, 5) for f in STAGE_FIXTURES] + [(f, 6) for f in STAGE_FIXTURES] +
-                         [(f, 7) for f in STAGE_FIXTURES])
+                         [(f, 7) for f in STAGE_FIXTURES] + [(f, 8) for f in STAGE_FIXTURES])
 def test_stages_match_oracle(have_gpu, name, mode):
     z = H.load(name)
     fl, sdf = make_fluid(z, mode)
@@ -309,7 +309,7 @@ def test_staged_blocks_fall_back_when_sparse(have_gpu):
     cfg.enable_scorr = 0
     cfg.particle_count = len(pos)
     outs = []
-    for mode in (4, 5, 7):
+    for mode in (4, 5, 7, 8):
         fl = P.PBFluids(cfg)
         fl.set_option(1, mode)
         fl.setParticles(P.make_particles(pos, vel))
@@ -327,7 +327,7 @@ def test_cooperative_and_per_thread_passes_agree(have_gpu):
     cfg, pos, vel = scenes.c0(16, seed=4)
     cfg.enable_scorr = 0
     outs = {}
-    for mode in (1, 0, 2, 2, 3, 3, 4, 5, 5, 6, 6, 7, 7):
+    for mode in (1, 0, 2, 2, 3, 3, 4, 5, 5, 6, 6, 7, 7, 8, 8):
         fl = P.PBFluids(cfg)
         fl.set_option(1, mode)
         fl.setParticles(P.make_particles(pos, vel))
@@ -337,7 +337,7 @@ def test_cooperative_and_per_thread_passes_agree(have_gpu):
             assert np.array_equal(outs[mode]["pos"], o["pos"]) and np.array_equal(outs[mode]["vel"], o["vel"])
         outs[mode] = o
     assert np.array_equal(outs[0]["pos"], outs[1]["pos"]) and np.array_equal(outs[0]["vel"], outs[1]["vel"])
-    for m in (2, 3, 4, 5, 6, 7):
+    for m in (2, 3, 4, 5, 6, 7, 8):
         assert np.abs(outs[m]["pos"] - outs[1]["pos"]).max() < 1e-5 * cfg.h
         assert np.abs(outs[m]["vel"] - outs[1]["vel"]).max() < 1e-3
 
@@ -385,5 +385,71 @@ def test_neighbour_list_overflow_falls_back(have_gpu):
     _, a = _run_mode(cfg, pos, vel, 4, 1)
     fl, b = _run_mode(cfg, pos, vel, 6, 1)
     assert fl.list_stats()[0] > 0
+    assert np.abs(a["pos"] - b["pos"]).max() < 1e-5 * cfg.h
+    assert np.abs(a["vel"] - b["vel"]).max() < 1e-3
+
+
+def _passes_per_step(cfg):
+    return cfg.substep_iterations * (2 * cfg.solver_iterations + 1) + (1 if cfg.enable_vorticity else 0)
+
+
+def test_dense_runs_agree_with_bucket_walk(have_gpu):
+    """Mode 8 (x-runs of the dense cell window, relabelled data).  With
+    s_corr on, over three steps, it is bit-identical to mode 6 (the same pair
+    arithmetic on the same relabelled arrays, pairs visited in the bucket
+    walk's order), although most particle passes take the runs in one and the
+    lists in the other.  (Against mode 4, whose integrate contracts one
+    velocity term differently, s_corr amplifies the last-bit differences over
+    steps, as it does for mode 6.)  In the smooth regime it matches mode 4
+    and most particle passes take the runs."""
+    cfg, pos, vel = scenes.c0(16, seed=6)
+    cfg.particle_count = len(pos)
+    _, a = _run_mode(cfg, pos, vel, 6, 3)
+    fl, b = _run_mode(cfg, pos, vel, 8, 3)
+    assert np.array_equal(a["pos"], b["pos"]) and np.array_equal(a["vel"], b["vel"])
+    _, c = _run_mode(cfg, pos, vel, 8, 3)  # deterministic
+    assert np.array_equal(b["pos"], c["pos"]) and np.array_equal(b["vel"], c["vel"])
+    cfg.enable_scorr = 0
+    _, a = _run_mode(cfg, pos, vel, 4, 3)
+    fl, b = _run_mode(cfg, pos, vel, 8, 3)
+    assert np.abs(a["pos"] - b["pos"]).max() < 1e-5 * cfg.h
+    assert np.abs(a["vel"] - b["vel"]).max() < 1e-3
+    walks, drifted, unclean = fl.list_stats()
+    assert drifted == 0 and walks < 0.3 * len(pos) * 3 * _passes_per_step(cfg)
+
+
+@pytest.mark.parametrize("hash_size", [64, 4096])
+def test_dense_runs_fall_back_on_hash_collisions(have_gpu, hash_size):
+    """A small hash table makes neighbouring cells share buckets, which the
+    reference then walks twice: cells with such a collision within two cells
+    walk the hashed buckets (64: all of them; 4096: some) and still match."""
+    cfg, pos, vel = scenes.c0(16, seed=2)
+    cfg.particle_count = len(pos)
+    cfg.hash_size = hash_size
+    cfg.enable_scorr = 0
+    _, a = _run_mode(cfg, pos, vel, 4, 2)
+    fl, b = _run_mode(cfg, pos, vel, 8, 2)
+    walks, drifted, unclean = fl.list_stats()
+    assert unclean > 0 and walks > 0
+    assert np.abs(a["pos"] - b["pos"]).max() < 1e-5 * cfg.h
+    assert np.abs(a["vel"] - b["vel"]).max() < 1e-3
+
+
+def test_dense_runs_drift_bound(have_gpu):
+    """Particles placed 1.5 h beyond the +x wall are clamped back by more than
+    the 0.9 h drift bound.  With a 4096-bucket table many cells have a
+    same-bucket cell within a few cells: those particles mark the cells within
+    their reach, whose queries walk the hashed buckets for the rest of the
+    substep, and the step still matches mode 4."""
+    cfg, pos, vel = scenes.c0(12, seed=3)
+    cfg.substep_iterations = 1
+    cfg.hash_size = 4096
+    pos = pos.copy()
+    pos[:50, 0] = cfg.bounds_max[0] + 1.5 * cfg.h
+    cfg.particle_count = len(pos)
+    _, a = _run_mode(cfg, pos, vel, 4, 1)
+    fl, b = _run_mode(cfg, pos, vel, 8, 1)
+    walks, marked, unclean = fl.list_stats()
+    assert marked > 0 and walks > 0
     assert np.abs(a["pos"] - b["pos"]).max() < 1e-5 * cfg.h
     assert np.abs(a["vel"] - b["vel"]).max() < 1e-3
