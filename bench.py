@@ -49,11 +49,11 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", type=int, default=4, choices=[0, 1, 2, 3, 4, 5, 6, 7, 8],
+    ap.add_argument("--mode", type=int, default=8, choices=[0, 1, 2, 3, 4, 5, 6, 7, 8],
                     help="neighbour passes: 0 hash order, 1 Morton, 2 Morton cell-cooperative, "
-                         "3 Morton with per-lane pair queues, 4 Morton with per-bucket hit masks (default), "
+                         "3 Morton with per-lane pair queues, 4 Morton with per-bucket hit masks, "
                          "5 Morton cell blocks staged through shared memory, 6 neighbour lists with a skin, "
-                         "7 per-block dense cell box in shared memory, 8 x-runs of a dense cell window")
+                         "7 per-block dense cell box in shared memory, 8 x-runs of a dense cell window (default)")
     ap.add_argument("--sample", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
                     help="smaller lattice of the same scene (profiling captures only)")
     return ap.parse_args()

@@ -286,10 +286,12 @@ int pbf_kernel_launches(pbf_handle* h, uint64_t* out);
  * parameter, particle or SDF change). */
 int pbf_set_use_graph(pbf_handle* h, int on);
 /* Execution options (results do not depend on them; no reference counterpart):
- *   PBF_OPT_SPATIAL_ORDER  4 (default): neighbour passes take particles in the
- *                          Morton order of their cells, one thread each, and
- *                          test each bucket in chunks of 8 before running the
- *                          pair body on the hits; 1: Morton order, body inside
+ *   PBF_OPT_SPATIAL_ORDER  8 (default), described last.  4: neighbour passes
+ *                          take particles in the Morton order of their cells,
+ *                          one thread each, and test each bucket in chunks of
+ *                          8 before running the pair body on the hits (the
+ *                          mode APBF and windows over 2^26 cells run under
+ *                          modes 6 and 8); 1: Morton order, body inside
  *                          the candidate loop; 2: Morton order, one warp per
  *                          cell with lanes sharing the candidate walk;
  *                          3: Morton order, in-range pairs queued per lane and
@@ -311,10 +313,12 @@ int pbf_set_use_graph(pbf_handle* h, int on);
  *                          range: 9 runs replace the 27 buckets wherever the
  *                          cell's neighbourhood has no hash collision and no
  *                          particle within reach has moved 0.9 h since the
- *                          predict; the hashed buckets elsewhere (APBF runs
- *                          mode 4).
- *                          Every mode gives the same results up to FP32
- *                          contraction differences.
+ *                          predict near a colliding cell; the hashed buckets
+ *                          elsewhere.  Same pairs, same order as the buckets.
+ *                          Modes 4, 6 and 8 give bit-identical results (same
+ *                          pairs, order and pair arithmetic); the others the
+ *                          same up to FP32 summation-order and contraction
+ *                          differences.
  *   PBF_OPT_LIST_SKIN      mode 6 list reach beyond h, in 1/1000 h (default 100). */
 #define PBF_OPT_SPATIAL_ORDER 1
 #define PBF_OPT_LIST_SKIN 2

@@ -1,7 +1,7 @@
 // k_dense.cu — neighbour mode 8: the hashed buckets replaced, where that is
 // exact, by runs of a dense cell window.
 //
-// The scene's box plus two cells on each side is a dense window of cells.
+// The scene's box plus a margin of cells on each side is a dense window.
 // After the hash sort of a substep, every particle is relabelled by the
 // window slot of its predict-time cell (z, then y, then x; cells outside the
 // window wrap into it) and the per-particle arrays are gathered into that
@@ -33,9 +33,10 @@
 // each particle now more than 0.9 h from its predict-time position: unless
 // that distance shows no colliding cell can be in a query's neighbourhood
 // (settle_drift), it marks the window cells within 1.01 h of where the
-// particle is ("dirty" for the rest of the substep): only a query in such a
-// cell can have it in range.  A
-// particle whose cell fails (a), (b) or (c) walks the 27 hashed buckets
+// particle is whose neighbourhood holds a colliding cell ("dirty" for the rest
+// of the substep): only a query in such a cell can see it through another
+// cell's bucket.  A particle whose cell fails (a), (b) or (c) walks the 27
+// hashed buckets
 // (through the hash-slot -> label map).  Both walks test candidates in chunks
 // into a hit mask exactly as the hashed-bucket passes do, so a pair's
 // arithmetic is the same in every walk.
@@ -103,6 +104,26 @@ __global__ void __launch_bounds__(128) k_d_clean(DenseArgs D, uint32_t mask, uin
     }
 }
 
+// Label range of the x-run centred on each window slot: slots s - 1, s, s + 1
+// of one row, (-1, -1) entries being empty cells; (0, 0) when all three are
+// empty and at the row ends (never walked: a walked cell is interior).
+__global__ void __launch_bounds__(256) k_d_runs(DenseArgs D, const int2* __restrict__ cells, int2* __restrict__ runs)
+{
+    const uint32_t slots = D.nx * D.ny * D.nz;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += stride) {
+        const uint32_t ux = s % D.nx;
+        int2 r = make_int2(0, 0);
+        if (ux >= 1 && ux + 1 < D.nx) {
+            const int2 e0 = __ldg(cells + s - 1), e1 = __ldg(cells + s), e2 = __ldg(cells + s + 1);
+            const int hi = max(max(e0.y, e1.y), e2.y);
+            // as unsigned, an empty cell's start (-1) is the largest
+            if (hi >= 0) r = make_int2((int)min(min((uint32_t)e0.x, (uint32_t)e1.x), (uint32_t)e2.x), hi);
+        }
+        runs[s] = r;
+    }
+}
+
 // Chebyshev distance from each window cell to the nearest other cell in the
 // same hash bucket, searched up to kDcolReach (kDcolReach + 1: none that near).
 constexpr int kDcolReach = 6;
@@ -135,15 +156,16 @@ __global__ void __launch_bounds__(128) k_d_dcol(DenseArgs D, uint32_t mask, uint
 // mask; the body runs for the hits in candidate order (masked_walk's scheme).
 // map(k) gives the label of candidate k (identity for a run; the hash-slot
 // -> label map for a bucket).
-template <class Map, class Hit, class Body>
+template <int C, class Map, class Hit, class Body>
 __device__ __forceinline__ void masked_range(const float4* __restrict__ X, float4 xi, int self, int lo, int hi,
                                              Map&& map, Hit&& hit, Body&& body)
 {
+    static_assert(C >= 1 && C <= 32, "hit mask is 32 bits");
 #pragma unroll 1
-    for (int k0 = lo; k0 < hi; k0 += kChunk) {
+    for (int k0 = lo; k0 < hi; k0 += C) {
         uint32_t m = 0;
 #pragma unroll
-        for (int c = 0; c < kChunk; ++c) {
+        for (int c = 0; c < C; ++c) {
             const int k = k0 + c;
             if (k < hi) {
                 const int j = map(k);
@@ -168,9 +190,12 @@ struct InvMap {
     __device__ __forceinline__ int operator()(int k) const { return (int)__ldg(inv + k); }
 };
 
+// Candidates per hit mask in a run (a run holds about 24).
+constexpr int kRunChunk = 16;
+
 // The 9 x-runs of a particle whose cell satisfies (a), (b) and (c).
 struct RunWalk {
-    const int2* __restrict__ table;
+    const int2* __restrict__ runs;
     const float4* __restrict__ X;
     float4 xi;
     int self;
@@ -183,13 +208,8 @@ struct RunWalk {
         for (int dz = -1; dz <= 1; ++dz) {
 #pragma unroll 1
             for (int dy = -1; dy <= 1; ++dy) {
-                const int s = s0 + dz * nxy + dy * nx;
-                const int2 e0 = __ldg(table + s - 1), e1 = __ldg(table + s), e2 = __ldg(table + s + 1);
-                const int hi = max(max(e0.y, e1.y), e2.y);
-                if (hi < 0) continue;
-                // empty slots hold (-1, -1): as unsigned their start is the largest
-                const int lo = (int)min(min((uint32_t)e0.x, (uint32_t)e1.x), (uint32_t)e2.x);
-                masked_range(X, xi, self, lo, hi, IdMap{}, hit, body);
+                const int2 r = __ldg(runs + s0 + dz * nxy + dy * nx);
+                masked_range<kRunChunk>(X, xi, self, r.x, r.y, IdMap{}, hit, body);
             }
         }
     }
@@ -217,7 +237,7 @@ struct BucketWalkLabels {
                 for (int dx = -1; dx <= 1; ++dx) {
                     const int2 se = __ldg(htable + ((((uint32_t)(cx + dx) * kP1) ^ hyz) & P.mask));
                     if (se.x == -1) continue;
-                    masked_range(X, xi, self, se.x, se.y, InvMap{inv}, hit, body);
+                    masked_range<kChunk>(X, xi, self, se.x, se.y, InvMap{inv}, hit, body);
                 }
             }
         }
@@ -236,7 +256,7 @@ __device__ __forceinline__ void with_dense_walker(const DevParams& P, const Dens
     if (ux - 1u < D.nx - 2u && uy - 1u < D.ny - 2u && uz - 1u < D.nz - 2u) {
         const int s0 = (int)((uz * D.ny + uy) * D.nx + ux);
         if (__ldg(D.clean + s0) && !D.dirty[s0]) {
-            core(RunWalk{D.table, X, xi, t, s0, (int)D.nx, (int)(D.nx * D.ny)});
+            core(RunWalk{D.runs, X, xi, t, s0, (int)D.nx, (int)(D.nx * D.ny)});
             return;
         }
     }
@@ -252,50 +272,58 @@ __device__ __forceinline__ void with_dense_walker(const DevParams& P, const Dens
 // queries lie within Chebyshev distance 2 of x's cell (1.01 h reach), their
 // neighbour cells within 3, so within 3 + cheb(cell(x), M) of M.  When M's
 // nearest same-bucket cell is farther (dcol), the particle is harmless;
-// otherwise the cells within reach of x are marked dirty.  Kept out of line:
-// it takes no registers from the passes.
-__device__ __noinline__ void settle_drift(const uint8_t* dcol, uint8_t* dirty, uint32_t* count, float h, float x,
-                                          float y, float z, float bx, float by, float bz, int gx0, int gy0, int gz0,
-                                          uint32_t nx, uint32_t ny, uint32_t nz)
+// otherwise every such N near the reach is found and the query cells within
+// reach that hold N, but not M, in their neighbourhood are marked dirty (a
+// query holding both has a collision in its neighbourhood and walks the
+// buckets anyway).  Kept out of line: it takes no registers from the passes.
+__device__ __noinline__ void settle_drift(const uint8_t* dcol, uint8_t* dirty, uint32_t* count, float h, uint32_t mask,
+                                          float x, float y, float z, float bx, float by, float bz, int gx0, int gy0,
+                                          int gz0, uint32_t nx, uint32_t ny, uint32_t nz)
 {
     const float c[3] = {x, y, z}, cb[3] = {bx, by, bz};
     const int g0[3] = {gx0, gy0, gz0};
     const uint32_t nd[3] = {nx, ny, nz};
-    long long cheb = 0;
+    long long m[3], rl[3], rh[3], cheb = 0;
     uint32_t um[3];
     bool inside = true;
+    const float r = 1.01f * h;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const int m = cell_coord(cb[a], h);
-        const long long d = (long long)cell_coord(c[a], h) - (long long)m;
+        m[a] = cell_coord(cb[a], h);
+        const long long d = (long long)cell_coord(c[a], h) - m[a];
         cheb = max(cheb, d < 0 ? -d : d);
-        um[a] = (uint32_t)m - (uint32_t)g0[a];
+        um[a] = (uint32_t)m[a] - (uint32_t)g0[a];
         inside = inside && um[a] < nd[a];
+        rl[a] = cell_coord(c[a] - r, h);
+        rh[a] = min((long long)cell_coord(c[a] + r, h), rl[a] + 3);
     }
     if (inside && cheb + 3 < (long long)dcol[(um[2] * ny + um[1]) * nx + um[0]]) return;
-    atomicAdd(count, 1u);
-    const float r = 1.01f * h;
-    uint32_t lo[3];
-    int cnt[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const int l = cell_coord(c[a] - r, h), hgh = cell_coord(c[a] + r, h);
-        const long long d = (long long)hgh - (long long)l;
-        cnt[a] = d < 0 ? 0 : (d > 3 ? 4 : (int)d + 1);
-        lo[a] = (uint32_t)l - (uint32_t)g0[a];
-    }
-    for (int iz = 0; iz < cnt[2]; ++iz) {
-        const uint32_t uz = lo[2] + (uint32_t)iz;
-        if (uz >= nz) continue;
-        for (int iy = 0; iy < cnt[1]; ++iy) {
-            const uint32_t uy = lo[1] + (uint32_t)iy;
-            if (uy >= ny) continue;
-            for (int ix = 0; ix < cnt[0]; ++ix) {
-                const uint32_t ux = lo[0] + (uint32_t)ix;
-                if (ux < nx) dirty[(uz * ny + uy) * nx + ux] = 1;
+    // Queries affected: cells q within reach of x whose neighbourhood holds
+    // a cell N != M of M's bucket but not M itself.  N then lies within one
+    // cell of the reach box.
+    const uint32_t hm = grid_hash((int)m[0], (int)m[1], (int)m[2], mask);
+    bool marked = false;
+    for (long long qz = rl[2] - 1; qz <= rh[2] + 1; ++qz)
+        for (long long qy = rl[1] - 1; qy <= rh[1] + 1; ++qy)
+            for (long long qx = rl[0] - 1; qx <= rh[0] + 1; ++qx) {
+                if ((qx == m[0] && qy == m[1] && qz == m[2]) ||
+                    grid_hash((int)(uint32_t)qx, (int)(uint32_t)qy, (int)(uint32_t)qz, mask) != hm)
+                    continue;
+                // N = (qx, qy, qz): mark reach cells within one cell of N and
+                // more than one cell from M
+                for (long long cz = max(rl[2], qz - 1); cz <= min(rh[2], qz + 1); ++cz)
+                    for (long long cy = max(rl[1], qy - 1); cy <= min(rh[1], qy + 1); ++cy)
+                        for (long long cx = max(rl[0], qx - 1); cx <= min(rh[0], qx + 1); ++cx) {
+                            const long long dm = max(max(cx - m[0], m[0] - cx), max(max(cy - m[1], m[1] - cy),
+                                                                                   max(cz - m[2], m[2] - cz)));
+                            if (dm <= 1) continue;
+                            const uint32_t ux = (uint32_t)cx - (uint32_t)g0[0], uy = (uint32_t)cy - (uint32_t)g0[1],
+                                           uz = (uint32_t)cz - (uint32_t)g0[2];
+                            if (ux < nx && uy < ny && uz < nz) dirty[(uz * ny + uy) * nx + ux] = 1;
+                            marked = true;
+                        }
             }
-        }
-    }
+    if (marked) atomicAdd(count, 1u);
 }
 
 __device__ __forceinline__ void check_drift(const DevParams& P, const DenseArgs& D, float4 x, int t)
@@ -304,7 +332,7 @@ __device__ __forceinline__ void check_drift(const DevParams& P, const DenseArgs&
     const float dx = x.x - b.x, dy = x.y - b.y, dz = x.z - b.z;
     // NaN positions count as moved (the comparison is false for NaN)
     if (!(dx * dx + dy * dy + dz * dz <= D.drift2))
-        settle_drift(D.dcol, D.dirty, D.flag, P.h, x.x, x.y, x.z, b.x, b.y, b.z, D.gx0, D.gy0, D.gz0, D.nx, D.ny,
+        settle_drift(D.dcol, D.dirty, D.flag, P.h, P.mask, x.x, x.y, x.z, b.x, b.y, b.z, D.gx0, D.gy0, D.gz0, D.nx, D.ny,
                      D.nz);
 }
 
@@ -323,7 +351,7 @@ __global__ void __launch_bounds__(kDThreads) k_d_lambda(DevParams P, DenseArgs D
     lrho[t] = rho;
 }
 
-__global__ void __launch_bounds__(kDThreads) k_d_deltap(DevParams P, DenseArgs D, const float4* __restrict__ lx_in,
+__global__ void __launch_bounds__(kDThreads, 10) k_d_deltap(DevParams P, DenseArgs D, const float4* __restrict__ lx_in,
                                                         float4* __restrict__ lx_out)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -337,7 +365,7 @@ __global__ void __launch_bounds__(kDThreads) k_d_deltap(DevParams P, DenseArgs D
     check_drift(P, D, out, t);
 }
 
-__global__ void __launch_bounds__(kDThreads) k_d_integrate(DevParams P, DenseArgs D, const float4* __restrict__ lx,
+__global__ void __launch_bounds__(kDThreads, 10) k_d_integrate(DevParams P, DenseArgs D, const float4* __restrict__ lx,
                                                            const float4* __restrict__ lv, float4* __restrict__ lx0,
                                                            float4* __restrict__ lom,
                                                            const uint32_t* __restrict__ lid, float4* __restrict__ pos,
@@ -397,6 +425,11 @@ void launch_d_keys(const DevParams& P, const DenseArgs& D, const float4* sx, uin
 void launch_d_clean(const DenseArgs& D, uint32_t mask, uint8_t* clean, uint32_t* unclean, int sms, cudaStream_t st)
 {
     k_d_clean<<<capped_grid(D.nx * D.ny * D.nz, 128, sms, 16), 128, 0, st>>>(D, mask, clean, unclean);
+}
+
+void launch_d_runs(const DenseArgs& D, const int2* cells, int2* runs, int sms, cudaStream_t st)
+{
+    k_d_runs<<<capped_grid(D.nx * D.ny * D.nz, 256, sms, 8), 256, 0, st>>>(D, cells, runs);
 }
 
 void launch_d_dcol(const DenseArgs& D, uint32_t mask, uint8_t* dcol, int sms, cudaStream_t st)

@@ -190,16 +190,17 @@ __device__ __forceinline__ float4 deltap_core(const DevParams& P, const SdfDev& 
              dy += ry * g;
              dz += rz * g;
          });
-    dx *= P.inv_rho0;
-    dy *= P.inv_rho0;
-    dz *= P.inv_rho0;
+    // rounded products (not fused into the x + dp below)
+    dx = __fmul_rn(dx, P.inv_rho0);
+    dy = __fmul_rn(dy, P.inv_rho0);
+    dz = __fmul_rn(dz, P.inv_rho0);
     dp_raw = make_float3(dx, dy, dz);
     const float l2 = dx * dx + dy * dy + dz * dz;
     if (l2 > P.max_dp * P.max_dp) {
         const float sc = P.max_dp * rsqrtf(l2);
-        dx *= sc;
-        dy *= sc;
-        dz *= sc;
+        dx = __fmul_rn(dx, sc);
+        dy = __fmul_rn(dy, sc);
+        dz = __fmul_rn(dz, sc);
     }
     float3 p = make_float3(xi.x + dx, xi.y + dy, xi.z + dz);
     if (sdf.enabled) {
@@ -251,18 +252,20 @@ __device__ __forceinline__ void integrate_core(const DevParams& P, const float* 
                  if (P.vort_on && r2 >= 1e-10f) {
                      const float sc = spiky_scale(P, r2);
                      const float ax = rx * sc, ay = ry * sc, az = rz * sc;
-                     cx += uy * az - uz * ay;
-                     cy += uz * ax - ux * az;
-                     cz += ux * ay - uy * ax;
+                     // a*b - c*d with the rounding fixed (one product rounded,
+                     // one fused), so every instantiation gives the same bits
+                     cx += __fmaf_rn(uy, az, -__fmul_rn(uz, ay));
+                     cy += __fmaf_rn(uz, ax, -__fmul_rn(ux, az));
+                     cz += __fmaf_rn(ux, ay, -__fmul_rn(uy, ax));
                  }
              });
     }
     float3 x = make_float3(x4.x, x4.y, x4.z);
     float vdx = 0.f, vdy = 0.f, vdz = 0.f;
     if (P.visc_on) {
-        vdx = fx * P.viscosity;
-        vdy = fy * P.viscosity;
-        vdz = fz * P.viscosity;
+        vdx = __fmul_rn(fx, P.viscosity);
+        vdy = __fmul_rn(fy, P.viscosity);
+        vdz = __fmul_rn(fz, P.viscosity);
     }
     if (P.vort_on) {
         const float ox = cx * P.inv_rho0, oy = cy * P.inv_rho0, oz = cz * P.inv_rho0;
@@ -278,9 +281,9 @@ __device__ __forceinline__ void integrate_core(const DevParams& P, const float* 
     bool col_sdf = false;
     float3 nrm = make_float3(0.0f, 0.0f, 0.0f);
     if (sdf.enabled) col_sdf = sdf_project(sdf, x, nrm);
-    float vx = (x.x - p0.x) * P.inv_dt + vdx;
-    float vy = (x.y - p0.y) * P.inv_dt + vdy;
-    float vz = (x.z - p0.z) * P.inv_dt + vdz;
+    float vx = __fmaf_rn(x.x - p0.x, P.inv_dt, vdx);
+    float vy = __fmaf_rn(x.y - p0.y, P.inv_dt, vdy);
+    float vz = __fmaf_rn(x.z - p0.z, P.inv_dt, vdz);
     const float sp2 = vx * vx + vy * vy + vz * vz;
     if (sp2 > 2500.0f) {
         const float sc = 50.0f / sqrtf(sp2);
@@ -348,8 +351,12 @@ __device__ __forceinline__ bool vorticity_core(const DevParams& P, XS X, MS OMAG
     const float el = sqrtf(ex * ex + ey * ey + ez * ez);
     if (el < 1e-6f) return false;
     const float nx = ex / el, ny = ey / el, nz = ez / el;
-    const float crx = ny * w.z - nz * w.y, cry = nz * w.x - nx * w.z, crz = nx * w.y - ny * w.x;
-    dv = make_float3(P.vort_eps * crx * P.dt, P.vort_eps * cry * P.dt, P.vort_eps * crz * P.dt);
+    const float crx = __fmaf_rn(ny, w.z, -__fmul_rn(nz, w.y)), cry = __fmaf_rn(nz, w.x, -__fmul_rn(nx, w.z)),
+                crz = __fmaf_rn(nx, w.y, -__fmul_rn(ny, w.x));
+    // rounded products: the caller adds dv to v, and a fused multiply-add
+    // there would round differently from one kernel to another
+    dv = make_float3(__fmul_rn(P.vort_eps * crx, P.dt), __fmul_rn(P.vort_eps * cry, P.dt),
+                     __fmul_rn(P.vort_eps * crz, P.dt));
     return true;
 }
 

@@ -317,7 +317,7 @@ pbf_handle::~pbf_handle()
     dfree(hist); dfree(totals); dfree(table); dfree(cand); dfree(ct_counts); dfree(scalars);
     dfree(lx[0]); dfree(lx[1]); dfree(lxb); dfree(lv); dfree(lx0); dfree(lom); dfree(lrho);
     dfree(lid); dfree(lkey); dfree(inv); dfree(list); dfree(lcnt); dfree(lstats); dfree(fastb);
-    dfree(dtable); dfree(dclean); dfree(ddcol); dfree(ddirty); dfree(dflag);
+    dfree(dtable); dfree(druns); dfree(dclean); dfree(ddcol); dfree(ddirty); dfree(dflag);
     dfree(grid); dfree(slab_min);
     mesh_free();
     if (stream) cudaStreamDestroy(stream);
@@ -407,9 +407,13 @@ int pbf_handle::ensure_label_capacity()
 
 // ---- dense cell window (mode 8) -----------------------------------------------------------
 // The walls' box in cells (floor(x / h) in FP32, as the kernels compute a
-// cell) with two cells of margin on each side.  Any window is correct (cells
-// outside wrap into it and their queries walk the hashed buckets); this one
-// puts every particle held by the walls in an interior cell.
+// cell) with kWindowMargin cells of margin on each side.  Any window is
+// correct (cells outside wrap into it and their queries walk the hashed
+// buckets); the margin also holds the predict-time cells of particles that
+// move towards a wall (x* = x + v dt lies beyond it until the walls clamp
+// it), whose later correction would otherwise count as an unchecked drift.
+constexpr int kWindowMargin = 6;
+
 bool pbf_handle::dense_window(int g0[3], uint32_t nd[3]) const
 {
     const float h = derived.h;
@@ -418,8 +422,8 @@ bool pbf_handle::dense_window(int g0[3], uint32_t nd[3]) const
     for (int a = 0; a < 3; ++a) {
         const float lo = std::floor(derived.bounds_min[a] / h), hi = std::floor(derived.bounds_max[a] / h);
         if (!(lo >= -1e8f && hi <= 1e8f && hi >= lo)) return false;
-        g0[a] = (int)lo - 2;
-        nd[a] = (uint32_t)((int)hi - (int)lo + 5);
+        g0[a] = (int)lo - kWindowMargin;
+        nd[a] = (uint32_t)((int)hi - (int)lo + 1 + 2 * kWindowMargin);
         slots *= nd[a];
     }
     return slots <= (1ull << 26);
@@ -429,6 +433,7 @@ DenseArgs pbf_handle::dense_args() const
 {
     DenseArgs D;
     D.table = dtable;
+    D.runs = druns;
     D.clean = dclean;
     D.dcol = ddcol;
     D.dirty = ddirty;
@@ -463,7 +468,8 @@ int pbf_handle::ensure_dense()
     if (same) return PBF_OK;
     if (capturing) return set_error(PBF_ERR_INVALID, "dense cell window changed during graph capture");
     if (slots > cap_slots || !dtable) {
-        if ((rc = dalloc(dtable, slots)) || (rc = dalloc(dclean, slots)) || (rc = dalloc(ddcol, slots)) ||
+        if ((rc = dalloc(dtable, slots)) || (rc = dalloc(druns, slots)) || (rc = dalloc(dclean, slots)) ||
+            (rc = dalloc(ddcol, slots)) ||
             (rc = dalloc(ddirty, slots)))
             return rc;
         cap_slots = slots;
@@ -648,7 +654,8 @@ int pbf_handle::stage(int st, uint32_t iter)
             ++launches;
             CK(cudaMemsetAsync(dtable, 0xFF, sizeof(int2) * slots, stream));
             launch_build_table(n, msorted, dtable, sms, stream);
-            ++launches;
+            launch_d_runs(dense_args(), dtable, druns, sms, stream);
+            launches += 2;
             CK(cudaMemsetAsync(ddirty, 0, slots, stream));
             CK(cudaMemsetAsync(dflag, 0, sizeof(uint32_t), stream));
             label_space = true;

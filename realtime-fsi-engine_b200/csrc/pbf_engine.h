@@ -42,8 +42,9 @@ struct pbf_handle {
     // spatial processing order of the neighbour passes (Morton order of the
     // predict-time cells); `order` points into one of the m* ping-pong pairs
     // PBF_OPT_SPATIAL_ORDER: 0 hash order, 1 Morton order, 2 Morton cell-cooperative,
-    // 3 Morton + per-lane pair queues, 4 Morton + per-bucket hit masks (default)
-    int pass_mode = 4;
+    // 3 Morton + per-lane pair queues, 4 Morton + per-bucket hit masks, 5-7 staged /
+    // listed variants, 8 x-runs of the dense cell window (default)
+    int pass_mode = 8;
     uint32_t *mcode = nullptr, *mka = nullptr, *mia = nullptr, *mkb = nullptr, *mib = nullptr;
     uint32_t* order = nullptr;
     // cell runs of the Morton order (one warp per run in the cooperative passes)
@@ -63,6 +64,7 @@ struct pbf_handle {
     uint32_t cap_label_n = 0;
     // mode 8: runs of a dense cell window (label arrays shared with mode 6)
     int2* dtable = nullptr;      // per window slot: label range
+    int2* druns = nullptr;       // per window slot: label range of its x-run (slots s-1 .. s+1)
     uint8_t* dclean = nullptr;   // per window slot: no hash collision near the cell
     uint8_t* ddcol = nullptr;    // per window slot: distance to the nearest other cell of its bucket
     uint8_t* ddirty = nullptr;   // per window slot: a moved particle within reach (per substep)
