@@ -49,11 +49,12 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", type=int, default=8, choices=[0, 1, 2, 3, 4, 5, 6, 7, 8],
-                    help="neighbour passes: 0 hash order, 1 Morton, 2 Morton cell-cooperative, "
-                         "3 Morton with per-lane pair queues, 4 Morton with per-bucket hit masks, "
-                         "5 Morton cell blocks staged through shared memory, 6 neighbour lists with a skin, "
-                         "7 per-block dense cell box in shared memory, 8 x-runs of a dense cell window (default)")
+    ap.add_argument("--mode", type=int, default=-1, choices=[-1, 0, 1, 2, 3, 4, 5, 6, 7, 8],
+                    help="neighbour passes: -1 automatic (default: 8 from 2^19 particles, else 4), 0 hash order, "
+                         "1 Morton, 2 Morton cell-cooperative, 3 Morton with per-lane pair queues, 4 Morton with "
+                         "per-bucket hit masks, 5 Morton cell blocks staged through shared memory, 6 neighbour "
+                         "lists with a skin, 7 per-block dense cell box in shared memory, 8 x-runs of a dense cell "
+                         "window")
     ap.add_argument("--sample", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
                     help="smaller lattice of the same scene (profiling captures only)")
     return ap.parse_args()
@@ -161,11 +162,12 @@ def peaks():
         return {}
 
 
-def traffic_summary():
-    """Per-launch DRAM bytes of the dominant kernel from a committed ncu
-    capture summary (profiles/traffic.json), scaled to the workload."""
+def traffic_summary(mode):
+    """DRAM bytes per particle of the neighbour passes of one neighbour mode,
+    from a committed ncu capture summary (profiles/traffic.json); the caller
+    scales them to the workload."""
     try:
-        return json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        return json.load(open(os.path.join(ROOT, "profiles", "traffic.json"))).get(str(mode), {})
     except Exception:
         return {}
 
@@ -259,7 +261,8 @@ def run_b200(args, dist):
     torch.cuda.synchronize(dev)
     clocks = Clocks(dev)
     l0 = fl.kernel_launches()
-    ws0 = fl.list_stats() if args.mode in (6, 7, 8) else None
+    mode = args.mode if args.mode >= 0 else (8 if n >= (1 << 19) else 4)
+    ws0 = fl.list_stats() if mode in (6, 7, 8) else None
     e0.record(stream)
     for _ in range(args.steps):
         fl.step()
@@ -309,7 +312,7 @@ def run_b200(args, dist):
                           "algo_bytes_per_launch": b,
                           "gbs": round(b / (per_launch / 1e3) / 1e9, 1) if per_launch > 0 else None}
     dom = max(per_pass, key=lambda k: per_pass[k]["ms_total"]) if per_pass else None
-    tr = traffic_summary().get(dom) if dom else None
+    tr = traffic_summary(mode).get(dom) if dom else None
     roof = None
     if dom:
         ach = per_pass[dom]["gbs"]
@@ -326,6 +329,7 @@ def run_b200(args, dist):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": desc, "particles_per_gpu": n, "substeps": subs,
                        "solver_iterations": cfg.solver_iterations, "hash_size": cfg.hash_size,
+                       "neighbour_mode": mode,
                        "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU",
                        "l2": "working set >> 126 MB L2 (no flush needed)"},
             "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
@@ -380,22 +384,29 @@ def run_batch(args, dist):
     value = n_all * subs * args.steps / (ms_max / 1e3)
 
     # the same scenes, one single-scene handle each, stepped one after the
-    # other (each scene's step completes before the next scene's starts)
-    seq = PB.make_sequential(cfg, mine, dev)
-    for f, _ in seq:
-        f.set_use_graph(True)
-    for _ in range(args.warmup):
+    # other (each scene's step completes before the next scene's starts), in
+    # the neighbour mode that is faster for them (the dense-window relabelling
+    # of mode 8 costs launches that small scenes do not earn back)
+    seq_by_mode = {}
+    for m in (4, 8):
+        seq = PB.make_sequential(cfg, mine, dev)
         for f, _ in seq:
-            f.step()
-            f.sync()
-    dist.barrier()
-    torch.cuda.synchronize(dev)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        for f, _ in seq:
-            f.step()
-            f.sync()
-    seq_s = dist.max(time.perf_counter() - t0)
+            f.set_option(1, m)
+            f.set_use_graph(True)
+        for _ in range(args.warmup):
+            for f, _ in seq:
+                f.step()
+                f.sync()
+        dist.barrier()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            for f, _ in seq:
+                f.step()
+                f.sync()
+        seq_by_mode[m] = (dist.max(time.perf_counter() - t0), seq)
+    seq_mode = min(seq_by_mode, key=lambda m: seq_by_mode[m][0])
+    seq_s, seq = seq_by_mode[seq_mode]
     seq_value = n_all * subs * args.steps / seq_s
     # accuracy: both forms advanced warmup + steps from the same state
     got = b.read_particles()
@@ -428,7 +439,9 @@ def run_batch(args, dist):
                        "l2": "working set > 126 MB L2 (no flush needed)"},
             "autotune": {"best": best, "candidates": cands},
             "sequential": {"value": seq_value, "ms_per_step": seq_s * 1e3 / args.steps,
-                           "form": "one PBFluids handle per scene (CUDA graph each), stepped one after another"},
+                           "form": "one PBFluids handle per scene (CUDA graph each), stepped one after another",
+                           "mode": seq_mode,
+                           "ms_per_step_by_mode": {str(m): v[0] * 1e3 / args.steps for m, v in seq_by_mode.items()}},
             "speedup_vs_sequential": value / seq_value,
             "max_pos_diff_vs_sequential": dmax,
             "e2e": {"value": n_all * subs * args.e2e_steps / e2e_s, "unit": METRIC, "h2d_bytes_per_step": n * 48,
@@ -436,7 +449,7 @@ def run_batch(args, dist):
             "roofline": None, "cpu_baseline": None, "gpu_launches": int(launches), "clocks": clk, "impl": "b200"}
     if dist.rank == 0:
         print(json.dumps(line), flush=True)
-    del seq
+    del seq, seq_by_mode
 
 
 def run_adjoint(args, dist):

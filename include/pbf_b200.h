@@ -286,7 +286,9 @@ int pbf_kernel_launches(pbf_handle* h, uint64_t* out);
  * parameter, particle or SDF change). */
 int pbf_set_use_graph(pbf_handle* h, int on);
 /* Execution options (results do not depend on them; no reference counterpart):
- *   PBF_OPT_SPATIAL_ORDER  8 (default), described last.  4: neighbour passes
+ *   PBF_OPT_SPATIAL_ORDER  -1 (default): mode 8 from 2^19 particles, mode 4
+ *                          below (where mode 8's relabelling launches cost
+ *                          more than its walk saves).  4: neighbour passes
  *                          take particles in the Morton order of their cells,
  *                          one thread each, and test each bucket in chunks of
  *                          8 before running the pair body on the hits (the

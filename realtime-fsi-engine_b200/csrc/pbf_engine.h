@@ -43,8 +43,9 @@ struct pbf_handle {
     // predict-time cells); `order` points into one of the m* ping-pong pairs
     // PBF_OPT_SPATIAL_ORDER: 0 hash order, 1 Morton order, 2 Morton cell-cooperative,
     // 3 Morton + per-lane pair queues, 4 Morton + per-bucket hit masks, 5-7 staged /
-    // listed variants, 8 x-runs of the dense cell window (default)
-    int pass_mode = 8;
+    // listed variants, 8 x-runs of the dense cell window; -1 (default): 8 from
+    // 2^19 particles, 4 below
+    int pass_mode = -1;
     uint32_t *mcode = nullptr, *mka = nullptr, *mia = nullptr, *mkb = nullptr, *mib = nullptr;
     uint32_t* order = nullptr;
     // cell runs of the Morton order (one warp per run in the cooperative passes)

@@ -449,3 +449,28 @@ def test_dense_runs_drift_bound(have_gpu):
     walks, marked, unclean = fl.list_stats()
     assert marked > 0 and walks > 0
     assert np.array_equal(a["pos"], b["pos"]) and np.array_equal(a["vel"], b["vel"])
+
+
+def test_automatic_mode_choice(have_gpu):
+    """The default neighbour mode is chosen by size: the dense-window runs
+    (mode 8, whose statistics report window cells) from 2^19 particles, the
+    masked bucket walk (mode 4, no statistics) below; both bit-identical to
+    the explicit modes."""
+    cfg, pos, vel, sdf = scenes.c2(nx=128, ny=64, nz=64)  # 524,288 particles
+    cfg.particle_count = len(pos)
+    _, a = _run_mode(cfg, pos, vel, -1, 1)
+    fl = P.PBFluids(cfg)
+    fl.setParticles(P.make_particles(pos, vel))
+    fl.step()
+    assert fl.list_stats()[2] > 0
+    _, b = _run_mode(cfg, pos, vel, 8, 1)
+    assert np.array_equal(a["pos"], b["pos"]) and np.array_equal(a["vel"], b["vel"])
+    cfg, pos, vel = scenes.c0(16)
+    cfg.particle_count = len(pos)
+    fl = P.PBFluids(cfg)
+    fl.setParticles(P.make_particles(pos, vel))
+    fl.step()
+    assert fl.list_stats() == (0, 0, 0)
+    _, b = _run_mode(cfg, pos, vel, 4, 1)
+    o = fl.readbackParticles()
+    assert np.array_equal(o["pos"], b["pos"]) and np.array_equal(o["vel"], b["vel"])
