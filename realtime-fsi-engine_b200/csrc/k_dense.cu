@@ -339,8 +339,9 @@ __device__ __forceinline__ void check_drift(const DevParams& P, const DenseArgs&
 __global__ void __launch_bounds__(kDThreads) k_d_lambda(DevParams P, DenseArgs D, const float4* __restrict__ lx_in,
                                                         float4* __restrict__ lx_out, float* __restrict__ lrho)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (int)P.n) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int)P.n) return;
+    const int t = D.order ? (int)__ldg(D.order + i) : i;
     const float4 xi = __ldg(lx_in + t);
     float rho, den;
     float3 g;
@@ -354,8 +355,9 @@ __global__ void __launch_bounds__(kDThreads) k_d_lambda(DevParams P, DenseArgs D
 __global__ void __launch_bounds__(kDThreads, 10) k_d_deltap(DevParams P, DenseArgs D, const float4* __restrict__ lx_in,
                                                         float4* __restrict__ lx_out)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (int)P.n) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int)P.n) return;
+    const int t = D.order ? (int)__ldg(D.order + i) : i;
     const float4 xi = __ldg(lx_in + t);
     float3 dp;
     float4 out;
@@ -371,8 +373,9 @@ __global__ void __launch_bounds__(kDThreads, 10) k_d_integrate(DevParams P, Dens
                                                            const uint32_t* __restrict__ lid, float4* __restrict__ pos,
                                                            float4* __restrict__ vel)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (int)P.n) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int)P.n) return;
+    const int t = D.order ? (int)__ldg(D.order + i) : i;
     const float4 x4 = __ldg(lx + t);
     const float4 v0 = __ldg(lv + t);
     const float4 p0 = lx0[t];
@@ -392,8 +395,9 @@ __global__ void __launch_bounds__(kDThreads) k_d_vorticity(DevParams P, DenseArg
                                                            const float4* __restrict__ lom,
                                                            const uint32_t* __restrict__ lid, float4* __restrict__ vel)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (int)P.n) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int)P.n) return;
+    const int t = D.order ? (int)__ldg(D.order + i) : i;
     const float4 xi = __ldg(lx0 + t);
     float3 dv;
     bool any = false;
@@ -407,6 +411,124 @@ __global__ void __launch_bounds__(kDThreads) k_d_vorticity(DevParams P, DenseArg
     v.y += dv.y;
     v.z += dv.z;
     vel[id] = v;
+}
+
+// ---- thread order by current cell ----------------------------------------------------------
+// The labels follow the predict-time cells; once the corrections have moved
+// particles, consecutive labels query different current cells and a warp's
+// candidate loads scatter.  Before a pass whose particles have moved, labels
+// are bucketed by the window slot of their current cell (counting sort: count,
+// scan, place); the pass's thread i then takes label order[i].  The order only
+// changes which thread computes which particle, never a result, so the place
+// step may use atomics in any order.
+constexpr uint32_t kScanItems = 4096;  // counters per block of the slot scan
+
+// slot of the current cell (cells outside the window interior: one extra slot)
+__global__ void __launch_bounds__(256) k_d_cslot(DevParams P, DenseArgs D, const float4* __restrict__ X,
+                                                 uint32_t* __restrict__ slot_of, uint32_t* __restrict__ cnt)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.n) return;
+    const float4 x = __ldg(X + t);
+    const uint32_t ux = (uint32_t)cell_coord(x.x, P.h) - (uint32_t)D.gx0;
+    const uint32_t uy = (uint32_t)cell_coord(x.y, P.h) - (uint32_t)D.gy0;
+    const uint32_t uz = (uint32_t)cell_coord(x.z, P.h) - (uint32_t)D.gz0;
+    const uint32_t slots = D.nx * D.ny * D.nz;
+    const uint32_t s = (ux < D.nx && uy < D.ny && uz < D.nz) ? (uz * D.ny + uy) * D.nx + ux : slots;
+    slot_of[t] = s;
+    const uint32_t peers = __match_any_sync(__activemask(), s);
+    if ((threadIdx.x & 31u) == (uint32_t)(__ffs(peers) - 1)) atomicAdd(cnt + s, (uint32_t)__popc(peers));
+}
+
+// exclusive scan of cnt[0 .. m) in place: per block of kScanItems, then the
+// block sums, then the block offsets
+__global__ void __launch_bounds__(1024) k_d_scan_blocks(uint32_t* __restrict__ cnt, uint32_t m,
+                                                        uint32_t* __restrict__ block_sums)
+{
+    __shared__ uint32_t warp_sums[32];
+    const uint32_t base = blockIdx.x * kScanItems + threadIdx.x * 4u;
+    uint32_t v[4], local = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        v[k] = base + k < m ? cnt[base + k] : 0u;
+        local += v[k];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t u = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += u;
+    }
+    if (lane == 31) warp_sums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = warp_sums[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t u = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += u;
+        }
+        warp_sums[lane] = w;
+    }
+    __syncthreads();
+    uint32_t run = incl - local + (warp ? warp_sums[warp - 1] : 0u);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (base + k < m) cnt[base + k] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == 1023) block_sums[blockIdx.x] = warp_sums[31];
+}
+
+__global__ void __launch_bounds__(1024) k_d_scan_sums(uint32_t* __restrict__ block_sums, uint32_t nb)
+{
+    __shared__ uint32_t warp_sums[32];
+    const uint32_t chunk = (nb + 1023u) / 1024u;
+    const uint32_t begin = threadIdx.x * chunk, end = min(begin + chunk, nb);
+    uint32_t local = 0;
+    for (uint32_t i = begin; i < end; ++i) local += block_sums[i];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t u = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += u;
+    }
+    if (lane == 31) warp_sums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = warp_sums[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t u = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += u;
+        }
+        warp_sums[lane] = w;
+    }
+    __syncthreads();
+    uint32_t run = incl - local + (warp ? warp_sums[warp - 1] : 0u);
+    for (uint32_t i = begin; i < end; ++i) {
+        const uint32_t v = block_sums[i];
+        block_sums[i] = run;
+        run += v;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_d_place(uint32_t n, const uint32_t* __restrict__ slot_of,
+                                                 uint32_t* __restrict__ start, const uint32_t* __restrict__ block_offs,
+                                                 uint32_t* __restrict__ order)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint32_t s = __ldg(slot_of + t);
+    const uint32_t peers = __match_any_sync(__activemask(), s);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t leader = (uint32_t)(__ffs(peers) - 1);
+    uint32_t b = 0;
+    if (lane == leader) b = atomicAdd(start + s, (uint32_t)__popc(peers));
+    b = __shfl_sync(peers, b, leader);
+    order[__ldg(block_offs + s / kScanItems) + b + __popc(peers & ((1u << lane) - 1u))] = t;
 }
 
 // ---- launchers ------------------------------------------------------------------------------
@@ -435,6 +557,22 @@ void launch_d_runs(const DenseArgs& D, const int2* cells, int2* runs, int sms, c
 void launch_d_dcol(const DenseArgs& D, uint32_t mask, uint8_t* dcol, int sms, cudaStream_t st)
 {
     k_d_dcol<<<capped_grid(D.nx * D.ny * D.nz, 128, sms, 16), 128, 0, st>>>(D, mask, dcol);
+}
+
+uint32_t order_scan_blocks(uint32_t slots) { return (slots + 1u + kScanItems - 1u) / kScanItems; }
+
+void launch_d_order(const DevParams& P, const DenseArgs& D, const float4* X, uint32_t* slot_of, uint32_t* cnt,
+                    uint32_t* block_sums, uint32_t* order, cudaStream_t st, uint64_t* launches)
+{
+    const uint32_t m = D.nx * D.ny * D.nz + 1u;  // slots + the outside slot
+    const uint32_t nb = order_scan_blocks(m - 1u);
+    cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * m, st);
+    const unsigned g = (P.n + 255u) / 256u;
+    k_d_cslot<<<g, 256, 0, st>>>(P, D, X, slot_of, cnt);
+    k_d_scan_blocks<<<nb, 1024, 0, st>>>(cnt, m, block_sums);
+    k_d_scan_sums<<<1, 1024, 0, st>>>(block_sums, nb);
+    k_d_place<<<g, 256, 0, st>>>(P.n, slot_of, cnt, block_sums, order);
+    *launches += 4;
 }
 
 void launch_d_lambda(const DevParams& P, const DenseArgs& D, const float4* lx_in, float4* lx_out, float* lrho,

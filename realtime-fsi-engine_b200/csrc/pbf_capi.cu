@@ -318,6 +318,7 @@ pbf_handle::~pbf_handle()
     dfree(lx[0]); dfree(lx[1]); dfree(lxb); dfree(lv); dfree(lx0); dfree(lom); dfree(lrho);
     dfree(lid); dfree(lkey); dfree(inv); dfree(list); dfree(lcnt); dfree(lstats); dfree(fastb);
     dfree(dtable); dfree(druns); dfree(dclean); dfree(ddcol); dfree(ddirty); dfree(dflag);
+    dfree(dslot); dfree(dord); dfree(dcnt); dfree(dbsum);
     dfree(grid); dfree(slab_min);
     mesh_free();
     if (stream) cudaStreamDestroy(stream);
@@ -438,6 +439,7 @@ DenseArgs pbf_handle::dense_args() const
     DenseArgs D;
     D.table = dtable;
     D.runs = druns;
+    D.order = nullptr;
     D.clean = dclean;
     D.dcol = ddcol;
     D.dirty = ddirty;
@@ -463,6 +465,12 @@ int pbf_handle::ensure_dense()
 {
     int rc;
     if ((rc = ensure_label_capacity())) return rc;
+    if (cap_ord_n < n || !dord) {
+        if (capturing) return set_error(PBF_ERR_INVALID, "particle count grew during graph capture");
+        const size_t c = std::max<uint32_t>(n, 1u);
+        if ((rc = dalloc(dslot, c)) || (rc = dalloc(dord, c))) return rc;
+        cap_ord_n = (uint32_t)c;
+    }
     int g0[3];
     uint32_t nd[3];
     if (!dense_window(g0, nd)) return set_error(PBF_ERR_INVALID, "dense cell window larger than 2^26 cells");
@@ -472,7 +480,8 @@ int pbf_handle::ensure_dense()
     if (same) return PBF_OK;
     if (capturing) return set_error(PBF_ERR_INVALID, "dense cell window changed during graph capture");
     if (slots > cap_slots || !dtable) {
-        if ((rc = dalloc(dtable, slots)) || (rc = dalloc(druns, slots)) || (rc = dalloc(dclean, slots)) ||
+        if ((rc = dalloc(dtable, slots)) || (rc = dalloc(druns, slots)) || (rc = dalloc(dcnt, slots + 1)) ||
+            (rc = dalloc(dbsum, order_scan_blocks((uint32_t)slots))) || (rc = dalloc(dclean, slots)) ||
             (rc = dalloc(ddcol, slots)) ||
             (rc = dalloc(ddirty, slots)))
             return rc;
@@ -593,21 +602,37 @@ int pbf_handle::stage(int st, uint32_t iter)
     }
     if (mode == 8 && st >= PBF_STAGE_LAMBDA && st <= PBF_STAGE_VORTICITY) {
         if (!label_space || !dwin_ready) return set_error(PBF_ERR_INVALID, "mode 8: run the reorder stage first");
-        const DenseArgs D = dense_args();
+        DenseArgs D = dense_args();
         prof_begin(st);
+        // after the first iteration the particles have moved off their
+        // predict-time cells: threads take them by current cell (lambda
+        // computes the order, the delta-p of the same iteration reuses it)
+        auto order_by = [&](const float4* X) {
+            launch_d_order(P, D, X, dslot, dcnt, dbsum, dord, stream, &launches);
+            D.order = dord;
+        };
         switch (st) {
         case PBF_STAGE_LAMBDA:
+            if (iter >= 2) {
+                order_by(lx[0]);
+                dord_iter = (int)iter;
+            }
             launch_d_lambda(P, D, lx[0], lx[1], lrho, stream);
             last_x = 1;
             break;
         case PBF_STAGE_DELTAP:
+            if (iter >= 2 && dord_iter == (int)iter) D.order = dord;
             launch_d_deltap(P, D, lx[1], lx[0], stream);
             last_x = 0;
             break;
         case PBF_STAGE_INTEGRATE:
+            order_by(lx[0]);
+            dord_iter = 0;
             launch_d_integrate(P, D, lx[0], lv, lx0, lom, lid, pos, vel, stream);
             break;
         default:
+            order_by(lx0);
+            dord_iter = 0;
             launch_d_vorticity(P, D, lx0, lom, lid, vel, stream);
             break;
         }
@@ -661,6 +686,7 @@ int pbf_handle::stage(int st, uint32_t iter)
             launch_d_runs(dense_args(), dtable, druns, sms, stream);
             launches += 2;
             CK(cudaMemsetAsync(ddirty, 0, slots, stream));
+            dord_iter = 0;
             CK(cudaMemsetAsync(dflag, 0, sizeof(uint32_t), stream));
             label_space = true;
             last_x = 0;

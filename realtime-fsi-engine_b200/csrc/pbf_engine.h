@@ -70,6 +70,10 @@ struct pbf_handle {
     uint8_t* ddcol = nullptr;    // per window slot: distance to the nearest other cell of its bucket
     uint8_t* ddirty = nullptr;   // per window slot: a moved particle within reach (per substep)
     uint32_t* dflag = nullptr;   // [0] drift-bound crossings, [1] bucket walks, [2] unclean slots
+    // thread order of the passes after particles have moved (labels by current cell)
+    uint32_t *dslot = nullptr, *dord = nullptr, *dcnt = nullptr, *dbsum = nullptr;
+    uint32_t cap_ord_n = 0;
+    int dord_iter = 0;           // solver iteration the order was computed for (0: none)
     size_t cap_slots = 0;
     int dwin_g0[3] = {0, 0, 0};
     uint32_t dwin_n[3] = {0, 0, 0};

@@ -131,6 +131,7 @@ void launch_l_unpermute1(uint32_t n, const uint32_t* inv, const float* src, floa
 struct DenseArgs {
     const int2* table;     // per window slot: label range of its particles, (-1, -1) when empty
     const int2* runs;      // per window slot: label range of slots s-1 .. s+1 of its row
+    const uint32_t* order; // pass thread i takes label order[i] (null: label i)
     const uint8_t* clean;  // per window slot: 1 = no hash collision near the cell
     const uint8_t* dcol;   // per window slot: Chebyshev distance to the nearest other cell of its bucket
     uint8_t* dirty;        // per window slot: a moved particle with a colliding cell near is within reach
@@ -146,6 +147,11 @@ void launch_d_keys(const DevParams& P, const DenseArgs& D, const float4* sx, uin
 void launch_d_clean(const DenseArgs& D, uint32_t mask, uint8_t* clean, uint32_t* unclean, int sms, cudaStream_t st);
 void launch_d_dcol(const DenseArgs& D, uint32_t mask, uint8_t* dcol, int sms, cudaStream_t st);
 void launch_d_runs(const DenseArgs& D, const int2* cells, int2* runs, int sms, cudaStream_t st);
+// Labels bucketed by the window slot of their current cell (X) into order[n].
+// Scratch: slot_of[n], cnt[slots + 1], block_sums[order_scan_blocks(slots)].
+uint32_t order_scan_blocks(uint32_t slots);
+void launch_d_order(const DevParams& P, const DenseArgs& D, const float4* X, uint32_t* slot_of, uint32_t* cnt,
+                    uint32_t* block_sums, uint32_t* order, cudaStream_t st, uint64_t* launches);
 void launch_d_lambda(const DevParams& P, const DenseArgs& D, const float4* lx_in, float4* lx_out, float* lrho,
                      cudaStream_t st);
 void launch_d_deltap(const DevParams& P, const DenseArgs& D, const float4* lx_in, float4* lx_out, cudaStream_t st);
