@@ -156,9 +156,13 @@ __global__ void __launch_bounds__(128) k_d_dcol(DenseArgs D, uint32_t mask, uint
 // mask; the body runs for the hits in candidate order (masked_walk's scheme).
 // map(k) gives the label of candidate k (identity for a run; the hash-slot
 // -> label map for a bucket).
-template <int C, class Map, class Hit, class Body>
+struct NoRecord {
+    __device__ __forceinline__ void operator()(uint32_t) const {}
+};
+
+template <int C, class Map, class Hit, class Body, class Rec = NoRecord>
 __device__ __forceinline__ void masked_range(const float4* __restrict__ X, float4 xi, int self, int lo, int hi,
-                                             Map&& map, Hit&& hit, Body&& body)
+                                             Map&& map, Hit&& hit, Body&& body, Rec&& rec = Rec{})
 {
     static_assert(C >= 1 && C <= 32, "hit mask is 32 bits");
 #pragma unroll 1
@@ -174,6 +178,7 @@ __device__ __forceinline__ void masked_range(const float4* __restrict__ X, float
                 if (hit(rx * rx + ry * ry + rz * rz) && j != self) m |= 1u << c;
             }
         }
+        rec(m);
         while (m) {
             const int c = __ffs(m) - 1;
             m &= m - 1u;
@@ -215,6 +220,91 @@ struct RunWalk {
     }
 };
 
+// Hit masks a lambda pass records for the delta-p pass of the same
+// iteration, which reads the same positions and so walks the same runs in the
+// same chunks and finds the same hits: word w of label t at hm[w * n + t], two
+// 16-bit chunk masks per word in walk order; the chunk count in cnt[t], or
+// kNoList when the particle walked the buckets or had more than kListChunks
+// chunks.  The delta-p pass then tests only the recorded hits (for its own
+// r >= 1e-10 condition) instead of every candidate.
+constexpr int kListWords = kDenseListWords;
+constexpr int kListChunks = 2 * kListWords;
+constexpr uint8_t kNoList = 0xFF;
+static_assert(kRunChunk == 16, "two chunk masks per list word");
+
+struct RunWalkRec {
+    const int2* __restrict__ runs;
+    const float4* __restrict__ X;
+    float4 xi;
+    int self;
+    int s0;
+    int nx, nxy;
+    uint32_t* __restrict__ hm;
+    uint32_t n;
+    int* chunks;
+    template <class Hit, class Body>
+    __device__ __forceinline__ void operator()(Hit&& hit, Body&& body) const
+    {
+        int q = 0;
+        uint32_t word = 0;
+#pragma unroll 1
+        for (int dz = -1; dz <= 1; ++dz) {
+#pragma unroll 1
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int2 r = __ldg(runs + s0 + dz * nxy + dy * nx);
+                masked_range<kRunChunk>(X, xi, self, r.x, r.y, IdMap{}, hit, body, [&](uint32_t m) {
+                    if (q < kListChunks) {
+                        if (q & 1)
+                            hm[(size_t)(q >> 1) * n + self] = word | (m << 16);
+                        else
+                            word = m;
+                    }
+                    ++q;
+                });
+            }
+        }
+        if (q <= kListChunks && (q & 1)) hm[(size_t)(q >> 1) * n + self] = word;
+        *chunks = q;
+    }
+};
+
+struct RunWalkList {
+    const int2* __restrict__ runs;
+    const float4* __restrict__ X;
+    float4 xi;
+    int self;
+    int s0;
+    int nx, nxy;
+    const uint32_t* __restrict__ hm;
+    uint32_t n;
+    template <class Hit, class Body>
+    __device__ __forceinline__ void operator()(Hit&& hit, Body&& body) const
+    {
+        int q = 0;
+        uint32_t word = 0;
+#pragma unroll 1
+        for (int dz = -1; dz <= 1; ++dz) {
+#pragma unroll 1
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int2 r = __ldg(runs + s0 + dz * nxy + dy * nx);
+#pragma unroll 1
+                for (int k0 = r.x; k0 < r.y; k0 += kRunChunk, ++q) {
+                    if ((q & 1) == 0) word = __ldg(hm + (size_t)(q >> 1) * n + self);
+                    uint32_t m = (q & 1) ? (word >> 16) : (word & 0xFFFFu);
+                    while (m) {
+                        const int c = __ffs(m) - 1;
+                        m &= m - 1u;
+                        const int k = k0 + c;
+                        const float4 xj = __ldg(X + k);
+                        const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+                        if (hit(rx * rx + ry * ry + rz * rz)) body(k);
+                    }
+                }
+            }
+        }
+    }
+};
+
 // The 27 hashed buckets in label space, in the reference's order.
 struct BucketWalkLabels {
     const DevParams& P;
@@ -244,24 +334,42 @@ struct BucketWalkLabels {
     }
 };
 
+// Window slot of the particle's current cell when its neighbourhood lies in
+// the window interior (else -1); fast_slot adds (b) and (c).
+__device__ __forceinline__ int interior_slot(const DevParams& P, const DenseArgs& D, float4 xi)
+{
+    const uint32_t ux = (uint32_t)cell_coord(xi.x, P.h) - (uint32_t)D.gx0;
+    const uint32_t uy = (uint32_t)cell_coord(xi.y, P.h) - (uint32_t)D.gy0;
+    const uint32_t uz = (uint32_t)cell_coord(xi.z, P.h) - (uint32_t)D.gz0;
+    if (ux - 1u < D.nx - 2u && uy - 1u < D.ny - 2u && uz - 1u < D.nz - 2u)
+        return (int)((uz * D.ny + uy) * D.nx + ux);
+    return -1;
+}
+
+__device__ __forceinline__ int fast_slot(const DevParams& P, const DenseArgs& D, float4 xi)
+{
+    const int s0 = interior_slot(P, D, xi);
+    return (s0 >= 0 && __ldg(D.clean + s0) && !D.dirty[s0]) ? s0 : -1;
+}
+
+__device__ __forceinline__ void count_bucket_walk(const DenseArgs& D)
+{
+    const uint32_t am = __activemask();
+    if ((threadIdx.x & 31u) == (uint32_t)(__ffs(am) - 1)) atomicAdd(D.flag + 1, (uint32_t)__popc(am));
+}
+
 // Run core(walker) with the run walk when (a), (b) and (c) hold, else with
 // the bucket walk.
 template <class Core>
 __device__ __forceinline__ void with_dense_walker(const DevParams& P, const DenseArgs& D, const float4* X, float4 xi,
                                                   int t, Core&& core)
 {
-    const uint32_t ux = (uint32_t)cell_coord(xi.x, P.h) - (uint32_t)D.gx0;
-    const uint32_t uy = (uint32_t)cell_coord(xi.y, P.h) - (uint32_t)D.gy0;
-    const uint32_t uz = (uint32_t)cell_coord(xi.z, P.h) - (uint32_t)D.gz0;
-    if (ux - 1u < D.nx - 2u && uy - 1u < D.ny - 2u && uz - 1u < D.nz - 2u) {
-        const int s0 = (int)((uz * D.ny + uy) * D.nx + ux);
-        if (__ldg(D.clean + s0) && !D.dirty[s0]) {
-            core(RunWalk{D.runs, X, xi, t, s0, (int)D.nx, (int)(D.nx * D.ny)});
-            return;
-        }
+    const int s0 = fast_slot(P, D, xi);
+    if (s0 >= 0) {
+        core(RunWalk{D.runs, X, xi, t, s0, (int)D.nx, (int)(D.nx * D.ny)});
+        return;
     }
-    const uint32_t am = __activemask();
-    if ((threadIdx.x & 31u) == (uint32_t)(__ffs(am) - 1)) atomicAdd(D.flag + 1, (uint32_t)__popc(am));
+    count_bucket_walk(D);
     core(BucketWalkLabels{P, D.htable, D.inv, X, xi, t});
 }
 
@@ -346,8 +454,18 @@ __global__ void __launch_bounds__(kDThreads) k_d_lambda(DevParams P, DenseArgs D
     float rho, den;
     float3 g;
     float4 out;
-    with_dense_walker(P, D, lx_in, xi, t,
-                      [&](auto&& walk) { out = lambda_core(P, GSrc{lx_in}, xi, walk, rho, g, den); });
+    const int s0 = fast_slot(P, D, xi);
+    if (s0 >= 0) {
+        int q = 0;
+        out = lambda_core(P, GSrc{lx_in}, xi,
+                          RunWalkRec{D.runs, lx_in, xi, t, s0, (int)D.nx, (int)(D.nx * D.ny), D.hm, P.n, &q}, rho, g,
+                          den);
+        D.hcnt[t] = q <= kListChunks ? (uint8_t)q : kNoList;
+    } else {
+        count_bucket_walk(D);
+        out = lambda_core(P, GSrc{lx_in}, xi, BucketWalkLabels{P, D.htable, D.inv, lx_in, xi, t}, rho, g, den);
+        D.hcnt[t] = kNoList;
+    }
     lx_out[t] = out;
     lrho[t] = rho;
 }
@@ -361,8 +479,15 @@ __global__ void __launch_bounds__(kDThreads, 10) k_d_deltap(DevParams P, DenseAr
     const float4 xi = __ldg(lx_in + t);
     float3 dp;
     float4 out;
-    with_dense_walker(P, D, lx_in, xi, t,
-                      [&](auto&& walk) { out = deltap_core(P, P.sdf, GSrc{lx_in}, xi, walk, dp); });
+    if (D.use_list && __ldg(D.hcnt + t) != kNoList) {
+        // the lambda pass of this iteration walked this particle's runs
+        const int s0 = interior_slot(P, D, xi);
+        out = deltap_core(P, P.sdf, GSrc{lx_in}, xi,
+                          RunWalkList{D.runs, lx_in, xi, t, s0, (int)D.nx, (int)(D.nx * D.ny), D.hm, P.n}, dp);
+    } else {
+        with_dense_walker(P, D, lx_in, xi, t,
+                          [&](auto&& walk) { out = deltap_core(P, P.sdf, GSrc{lx_in}, xi, walk, dp); });
+    }
     lx_out[t] = out;
     check_drift(P, D, out, t);
 }

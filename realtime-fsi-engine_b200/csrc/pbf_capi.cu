@@ -318,7 +318,7 @@ pbf_handle::~pbf_handle()
     dfree(lx[0]); dfree(lx[1]); dfree(lxb); dfree(lv); dfree(lx0); dfree(lom); dfree(lrho);
     dfree(lid); dfree(lkey); dfree(inv); dfree(list); dfree(lcnt); dfree(lstats); dfree(fastb);
     dfree(dtable); dfree(druns); dfree(dclean); dfree(ddcol); dfree(ddirty); dfree(dflag);
-    dfree(dslot); dfree(dord); dfree(dcnt); dfree(dbsum);
+    dfree(dslot); dfree(dord); dfree(dcnt); dfree(dbsum); dfree(dhm); dfree(dhcnt);
     dfree(grid); dfree(slab_min);
     mesh_free();
     if (stream) cudaStreamDestroy(stream);
@@ -440,6 +440,9 @@ DenseArgs pbf_handle::dense_args() const
     D.table = dtable;
     D.runs = druns;
     D.order = nullptr;
+    D.hm = dhm;
+    D.hcnt = dhcnt;
+    D.use_list = 0;
     D.clean = dclean;
     D.dcol = ddcol;
     D.dirty = ddirty;
@@ -468,7 +471,9 @@ int pbf_handle::ensure_dense()
     if (cap_ord_n < n || !dord) {
         if (capturing) return set_error(PBF_ERR_INVALID, "particle count grew during graph capture");
         const size_t c = std::max<uint32_t>(n, 1u);
-        if ((rc = dalloc(dslot, c)) || (rc = dalloc(dord, c))) return rc;
+        if ((rc = dalloc(dslot, c)) || (rc = dalloc(dord, c)) || (rc = dalloc(dhm, c * kDenseListWords)) ||
+            (rc = dalloc(dhcnt, c)))
+            return rc;
         cap_ord_n = (uint32_t)c;
     }
     int g0[3];
@@ -618,16 +623,20 @@ int pbf_handle::stage(int st, uint32_t iter)
                 dord_iter = (int)iter;
             }
             launch_d_lambda(P, D, lx[0], lx[1], lrho, stream);
+            dlist_iter = (int)iter;
             last_x = 1;
             break;
         case PBF_STAGE_DELTAP:
             if (iter >= 2 && dord_iter == (int)iter) D.order = dord;
+            D.use_list = dlist_iter == (int)iter ? 1 : 0;
+            dlist_iter = 0;
             launch_d_deltap(P, D, lx[1], lx[0], stream);
             last_x = 0;
             break;
         case PBF_STAGE_INTEGRATE:
             order_by(lx[0]);
             dord_iter = 0;
+            dlist_iter = 0;
             launch_d_integrate(P, D, lx[0], lv, lx0, lom, lid, pos, vel, stream);
             break;
         default:
@@ -687,6 +696,7 @@ int pbf_handle::stage(int st, uint32_t iter)
             launches += 2;
             CK(cudaMemsetAsync(ddirty, 0, slots, stream));
             dord_iter = 0;
+            dlist_iter = 0;
             CK(cudaMemsetAsync(dflag, 0, sizeof(uint32_t), stream));
             label_space = true;
             last_x = 0;

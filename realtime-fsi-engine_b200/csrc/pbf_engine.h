@@ -74,6 +74,10 @@ struct pbf_handle {
     uint32_t *dslot = nullptr, *dord = nullptr, *dcnt = nullptr, *dbsum = nullptr;
     uint32_t cap_ord_n = 0;
     int dord_iter = 0;           // solver iteration the order was computed for (0: none)
+    // lambda hit masks replayed by the delta-p pass of the same iteration
+    uint32_t* dhm = nullptr;
+    uint8_t* dhcnt = nullptr;
+    int dlist_iter = 0;          // solver iteration whose lambda recorded them (0: none)
     size_t cap_slots = 0;
     int dwin_g0[3] = {0, 0, 0};
     uint32_t dwin_n[3] = {0, 0, 0};

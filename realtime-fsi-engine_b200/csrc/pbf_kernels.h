@@ -128,10 +128,14 @@ void launch_l_unpermute4(uint32_t n, const uint32_t* inv, const float4* src, flo
 void launch_l_unpermute1(uint32_t n, const uint32_t* inv, const float* src, float* dst, int sms, cudaStream_t st);
 
 // ---- k_dense.cu: x-runs of a dense cell window over relabelled data ----------
+constexpr int kDenseListWords = 16;
 struct DenseArgs {
     const int2* table;     // per window slot: label range of its particles, (-1, -1) when empty
     const int2* runs;      // per window slot: label range of slots s-1 .. s+1 of its row
     const uint32_t* order; // pass thread i takes label order[i] (null: label i)
+    uint32_t* hm;          // lambda hit masks for the delta-p of the same iteration (kDenseListWords x n)
+    uint8_t* hcnt;         // per label: chunks recorded, 0xFF = none
+    int use_list;          // delta-p: the lambda pass of this iteration recorded hm/hcnt
     const uint8_t* clean;  // per window slot: 1 = no hash collision near the cell
     const uint8_t* dcol;   // per window slot: Chebyshev distance to the nearest other cell of its bucket
     uint8_t* dirty;        // per window slot: a moved particle with a colliding cell near is within reach
