@@ -277,20 +277,33 @@ struct RunWalkList {
     int nx, nxy;
     const uint32_t* __restrict__ hm;
     uint32_t n;
+    __device__ __forceinline__ uint32_t chunk_mask(int q) const
+    {
+        const uint32_t w = __ldg(hm + (size_t)(q >> 1) * n + self);
+        return (q & 1) ? (w >> 16) : (w & 0xFFFFu);
+    }
+    // Two consecutive chunks of a run (32 consecutive candidates) are drained
+    // as one 32-bit mask: a warp then runs the pair body as many times as its
+    // busiest lane has hits among 32 candidates rather than 16 twice over.
     template <class Hit, class Body>
     __device__ __forceinline__ void operator()(Hit&& hit, Body&& body) const
     {
         int q = 0;
-        uint32_t word = 0;
 #pragma unroll 1
         for (int dz = -1; dz <= 1; ++dz) {
 #pragma unroll 1
             for (int dy = -1; dy <= 1; ++dy) {
                 const int2 r = __ldg(runs + s0 + dz * nxy + dy * nx);
 #pragma unroll 1
-                for (int k0 = r.x; k0 < r.y; k0 += kRunChunk, ++q) {
-                    if ((q & 1) == 0) word = __ldg(hm + (size_t)(q >> 1) * n + self);
-                    uint32_t m = (q & 1) ? (word >> 16) : (word & 0xFFFFu);
+                for (int k0 = r.x; k0 < r.y; k0 += 2 * kRunChunk) {
+                    uint32_t m;
+                    if ((q & 1) == 0 && k0 + kRunChunk < r.y) {
+                        m = __ldg(hm + (size_t)(q >> 1) * n + self);  // both halves belong to this run
+                        q += 2;
+                    } else {
+                        m = chunk_mask(q++);
+                        if (k0 + kRunChunk < r.y) m |= chunk_mask(q++) << 16;
+                    }
                     while (m) {
                         const int c = __ffs(m) - 1;
                         m &= m - 1u;
