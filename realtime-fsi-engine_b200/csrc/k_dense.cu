@@ -561,21 +561,39 @@ __global__ void __launch_bounds__(kDThreads) k_d_vorticity(DevParams P, DenseArg
 // step may use atomics in any order.
 constexpr uint32_t kScanItems = 4096;  // counters per block of the slot scan
 
+// Runs of equal slots among the lanes of a warp (lanes hold consecutive
+// labels, mostly of one cell): the lane that heads this lane's run and the
+// run's length.
+__device__ __forceinline__ void slot_run(uint32_t s, uint32_t lane, uint32_t& head, uint32_t& len)
+{
+    const uint32_t prev = __shfl_up_sync(0xffffffffu, s, 1);
+    const uint32_t heads = __ballot_sync(0xffffffffu, lane == 0u || prev != s);
+    head = 31u - (uint32_t)__clz(heads & (0xffffffffu >> (31u - lane)));
+    const uint32_t after = heads & ~(0xffffffffu >> (31u - head));
+    len = (after ? (uint32_t)(__ffs(after) - 1) : 32u) - head;
+}
+
+constexpr uint32_t kNoSlot = 0xffffffffu;
+
 // slot of the current cell (cells outside the window interior: one extra slot)
 __global__ void __launch_bounds__(256) k_d_cslot(DevParams P, DenseArgs D, const float4* __restrict__ X,
                                                  uint32_t* __restrict__ slot_of, uint32_t* __restrict__ cnt)
 {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= P.n) return;
-    const float4 x = __ldg(X + t);
-    const uint32_t ux = (uint32_t)cell_coord(x.x, P.h) - (uint32_t)D.gx0;
-    const uint32_t uy = (uint32_t)cell_coord(x.y, P.h) - (uint32_t)D.gy0;
-    const uint32_t uz = (uint32_t)cell_coord(x.z, P.h) - (uint32_t)D.gz0;
-    const uint32_t slots = D.nx * D.ny * D.nz;
-    const uint32_t s = (ux < D.nx && uy < D.ny && uz < D.nz) ? (uz * D.ny + uy) * D.nx + ux : slots;
-    slot_of[t] = s;
-    const uint32_t peers = __match_any_sync(__activemask(), s);
-    if ((threadIdx.x & 31u) == (uint32_t)(__ffs(peers) - 1)) atomicAdd(cnt + s, (uint32_t)__popc(peers));
+    uint32_t s = kNoSlot;
+    if (t < P.n) {
+        const float4 x = __ldg(X + t);
+        const uint32_t ux = (uint32_t)cell_coord(x.x, P.h) - (uint32_t)D.gx0;
+        const uint32_t uy = (uint32_t)cell_coord(x.y, P.h) - (uint32_t)D.gy0;
+        const uint32_t uz = (uint32_t)cell_coord(x.z, P.h) - (uint32_t)D.gz0;
+        const uint32_t slots = D.nx * D.ny * D.nz;
+        s = (ux < D.nx && uy < D.ny && uz < D.nz) ? (uz * D.ny + uy) * D.nx + ux : slots;
+        slot_of[t] = s;
+    }
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t head, len;
+    slot_run(s, lane, head, len);
+    if (lane == head && s != kNoSlot) atomicAdd(cnt + s, len);
 }
 
 // exclusive scan of cnt[0 .. m) in place: per block of kScanItems, then the
@@ -658,15 +676,14 @@ __global__ void __launch_bounds__(256) k_d_place(uint32_t n, const uint32_t* __r
                                                  uint32_t* __restrict__ order)
 {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const uint32_t s = __ldg(slot_of + t);
-    const uint32_t peers = __match_any_sync(__activemask(), s);
+    const uint32_t s = t < n ? __ldg(slot_of + t) : kNoSlot;
     const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t leader = (uint32_t)(__ffs(peers) - 1);
+    uint32_t head, len;
+    slot_run(s, lane, head, len);
     uint32_t b = 0;
-    if (lane == leader) b = atomicAdd(start + s, (uint32_t)__popc(peers));
-    b = __shfl_sync(peers, b, leader);
-    order[__ldg(block_offs + s / kScanItems) + b + __popc(peers & ((1u << lane) - 1u))] = t;
+    if (lane == head && s != kNoSlot) b = atomicAdd(start + s, len);
+    b = __shfl_sync(0xffffffffu, b, head);
+    if (s != kNoSlot) order[__ldg(block_offs + s / kScanItems) + b + (lane - head)] = t;
 }
 
 // ---- launchers ------------------------------------------------------------------------------
