@@ -457,100 +457,6 @@ __device__ __forceinline__ void check_drift(const DevParams& P, const DenseArgs&
                      D.nz);
 }
 
-__global__ void __launch_bounds__(kDThreads) k_d_lambda(DevParams P, DenseArgs D, const float4* __restrict__ lx_in,
-                                                        float4* __restrict__ lx_out, float* __restrict__ lrho)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (int)P.n) return;
-    const int t = D.order ? (int)__ldg(D.order + i) : i;
-    const float4 xi = __ldg(lx_in + t);
-    float rho, den;
-    float3 g;
-    float4 out;
-    const int s0 = fast_slot(P, D, xi);
-    if (s0 >= 0) {
-        int q = 0;
-        out = lambda_core(P, GSrc{lx_in}, xi,
-                          RunWalkRec{D.runs, lx_in, xi, t, s0, (int)D.nx, (int)(D.nx * D.ny), D.hm, P.n, &q}, rho, g,
-                          den);
-        D.hcnt[t] = q <= kListChunks ? (uint8_t)q : kNoList;
-    } else {
-        count_bucket_walk(D);
-        out = lambda_core(P, GSrc{lx_in}, xi, BucketWalkLabels{P, D.htable, D.inv, lx_in, xi, t}, rho, g, den);
-        D.hcnt[t] = kNoList;
-    }
-    lx_out[t] = out;
-    lrho[t] = rho;
-}
-
-__global__ void __launch_bounds__(kDThreads, 10) k_d_deltap(DevParams P, DenseArgs D, const float4* __restrict__ lx_in,
-                                                        float4* __restrict__ lx_out)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (int)P.n) return;
-    const int t = D.order ? (int)__ldg(D.order + i) : i;
-    const float4 xi = __ldg(lx_in + t);
-    float3 dp;
-    float4 out;
-    if (D.use_list && __ldg(D.hcnt + t) != kNoList) {
-        // the lambda pass of this iteration walked this particle's runs
-        const int s0 = interior_slot(P, D, xi);
-        out = deltap_core(P, P.sdf, GSrc{lx_in}, xi,
-                          RunWalkList{D.runs, lx_in, xi, t, s0, (int)D.nx, (int)(D.nx * D.ny), D.hm, P.n}, dp);
-    } else {
-        with_dense_walker(P, D, lx_in, xi, t,
-                          [&](auto&& walk) { out = deltap_core(P, P.sdf, GSrc{lx_in}, xi, walk, dp); });
-    }
-    lx_out[t] = out;
-    check_drift(P, D, out, t);
-}
-
-__global__ void __launch_bounds__(kDThreads, 10) k_d_integrate(DevParams P, DenseArgs D, const float4* __restrict__ lx,
-                                                           const float4* __restrict__ lv, float4* __restrict__ lx0,
-                                                           float4* __restrict__ lom,
-                                                           const uint32_t* __restrict__ lid, float4* __restrict__ pos,
-                                                           float4* __restrict__ vel)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (int)P.n) return;
-    const int t = D.order ? (int)__ldg(D.order + i) : i;
-    const float4 x4 = __ldg(lx + t);
-    const float4 v0 = __ldg(lv + t);
-    const float4 p0 = lx0[t];
-    float4 xo, vo, om;
-    with_dense_walker(P, D, lx, x4, t, [&](auto&& walk) {
-        integrate_core(P, P.bmin, P.bmax, P.sdf, GSrc{lx}, GSrc{lv}, x4, v0, p0, walk, xo, vo, om);
-    });
-    if (P.vort_on) lom[t] = om;
-    const uint32_t id = __ldg(lid + t);
-    pos[id] = xo;
-    vel[id] = vo;
-    lx0[t] = xo;
-    check_drift(P, D, xo, t);
-}
-
-__global__ void __launch_bounds__(kDThreads) k_d_vorticity(DevParams P, DenseArgs D, const float4* __restrict__ lx0,
-                                                           const float4* __restrict__ lom,
-                                                           const uint32_t* __restrict__ lid, float4* __restrict__ vel)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (int)P.n) return;
-    const int t = D.order ? (int)__ldg(D.order + i) : i;
-    const float4 xi = __ldg(lx0 + t);
-    float3 dv;
-    bool any = false;
-    with_dense_walker(P, D, lx0, xi, t, [&](auto&& walk) {
-        any = vorticity_core(P, GSrc{lx0}, GMag{lom}, xi, __ldg(lom + t), walk, dv);
-    });
-    if (!any) return;
-    const uint32_t id = __ldg(lid + t);
-    float4 v = vel[id];
-    v.x += dv.x;
-    v.y += dv.y;
-    v.z += dv.z;
-    vel[id] = v;
-}
-
 // ---- thread order by current cell ----------------------------------------------------------
 // The labels follow the predict-time cells; once the corrections have moved
 // particles, consecutive labels query different current cells and a warp's
@@ -594,6 +500,25 @@ __global__ void __launch_bounds__(256) k_d_cslot(DevParams P, DenseArgs D, const
     uint32_t head, len;
     slot_run(s, lane, head, len);
     if (lane == head && s != kNoSlot) atomicAdd(cnt + s, len);
+}
+
+// The slot a pass's output position falls in, recorded for the thread order
+// of the next pass (k_d_cslot's work folded into the pass that moves the
+// particle).  Every lane of the warp calls it; valid = the lane has a particle.
+__device__ __forceinline__ void record_slot(const DevParams& P, const DenseArgs& D, float4 x, int t, bool valid)
+{
+    uint32_t s = kNoSlot;
+    if (valid) {
+        const uint32_t ux = (uint32_t)cell_coord(x.x, P.h) - (uint32_t)D.gx0;
+        const uint32_t uy = (uint32_t)cell_coord(x.y, P.h) - (uint32_t)D.gy0;
+        const uint32_t uz = (uint32_t)cell_coord(x.z, P.h) - (uint32_t)D.gz0;
+        s = (ux < D.nx && uy < D.ny && uz < D.nz) ? (uz * D.ny + uy) * D.nx + ux : D.nx * D.ny * D.nz;
+        D.rec_slot[t] = s;
+    }
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t head, len;
+    slot_run(s, lane, head, len);
+    if (lane == head && s != kNoSlot) atomicAdd(D.rec_cnt + s, len);
 }
 
 // exclusive scan of cnt[0 .. m) in place: per block of kScanItems, then the
@@ -686,6 +611,107 @@ __global__ void __launch_bounds__(256) k_d_place(uint32_t n, const uint32_t* __r
     if (s != kNoSlot) order[__ldg(block_offs + s / kScanItems) + b + (lane - head)] = t;
 }
 
+__global__ void __launch_bounds__(kDThreads) k_d_lambda(DevParams P, DenseArgs D, const float4* __restrict__ lx_in,
+                                                        float4* __restrict__ lx_out, float* __restrict__ lrho)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int)P.n) return;
+    const int t = D.order ? (int)__ldg(D.order + i) : i;
+    const float4 xi = __ldg(lx_in + t);
+    float rho, den;
+    float3 g;
+    float4 out;
+    const int s0 = fast_slot(P, D, xi);
+    if (s0 >= 0) {
+        int q = 0;
+        out = lambda_core(P, GSrc{lx_in}, xi,
+                          RunWalkRec{D.runs, lx_in, xi, t, s0, (int)D.nx, (int)(D.nx * D.ny), D.hm, P.n, &q}, rho, g,
+                          den);
+        D.hcnt[t] = q <= kListChunks ? (uint8_t)q : kNoList;
+    } else {
+        count_bucket_walk(D);
+        out = lambda_core(P, GSrc{lx_in}, xi, BucketWalkLabels{P, D.htable, D.inv, lx_in, xi, t}, rho, g, den);
+        D.hcnt[t] = kNoList;
+    }
+    lx_out[t] = out;
+    lrho[t] = rho;
+}
+
+__global__ void __launch_bounds__(kDThreads, 10) k_d_deltap(DevParams P, DenseArgs D, const float4* __restrict__ lx_in,
+                                                        float4* __restrict__ lx_out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < (int)P.n;
+    const int t = live ? (D.order ? (int)__ldg(D.order + i) : i) : 0;
+    float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (live) {
+        const float4 xi = __ldg(lx_in + t);
+        float3 dp;
+        if (D.use_list && __ldg(D.hcnt + t) != kNoList) {
+            // the lambda pass of this iteration walked this particle's runs
+            const int s0 = interior_slot(P, D, xi);
+            out = deltap_core(P, P.sdf, GSrc{lx_in}, xi,
+                              RunWalkList{D.runs, lx_in, xi, t, s0, (int)D.nx, (int)(D.nx * D.ny), D.hm, P.n}, dp);
+        } else {
+            with_dense_walker(P, D, lx_in, xi, t,
+                              [&](auto&& walk) { out = deltap_core(P, P.sdf, GSrc{lx_in}, xi, walk, dp); });
+        }
+        lx_out[t] = out;
+        check_drift(P, D, out, t);
+    }
+    if (D.rec_cnt) record_slot(P, D, out, t, live);
+}
+
+__global__ void __launch_bounds__(kDThreads, 10) k_d_integrate(DevParams P, DenseArgs D, const float4* __restrict__ lx,
+                                                           const float4* __restrict__ lv, float4* __restrict__ lx0,
+                                                           float4* __restrict__ lom,
+                                                           const uint32_t* __restrict__ lid, float4* __restrict__ pos,
+                                                           float4* __restrict__ vel)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < (int)P.n;
+    const int t = live ? (D.order ? (int)__ldg(D.order + i) : i) : 0;
+    float4 xo = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (live) {
+        const float4 x4 = __ldg(lx + t);
+        const float4 v0 = __ldg(lv + t);
+        const float4 p0 = lx0[t];
+        float4 vo, om;
+        with_dense_walker(P, D, lx, x4, t, [&](auto&& walk) {
+            integrate_core(P, P.bmin, P.bmax, P.sdf, GSrc{lx}, GSrc{lv}, x4, v0, p0, walk, xo, vo, om);
+        });
+        if (P.vort_on) lom[t] = om;
+        const uint32_t id = __ldg(lid + t);
+        pos[id] = xo;
+        vel[id] = vo;
+        lx0[t] = xo;
+        check_drift(P, D, xo, t);
+    }
+    if (D.rec_cnt) record_slot(P, D, xo, t, live);
+}
+
+__global__ void __launch_bounds__(kDThreads) k_d_vorticity(DevParams P, DenseArgs D, const float4* __restrict__ lx0,
+                                                           const float4* __restrict__ lom,
+                                                           const uint32_t* __restrict__ lid, float4* __restrict__ vel)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int)P.n) return;
+    const int t = D.order ? (int)__ldg(D.order + i) : i;
+    const float4 xi = __ldg(lx0 + t);
+    float3 dv;
+    bool any = false;
+    with_dense_walker(P, D, lx0, xi, t, [&](auto&& walk) {
+        any = vorticity_core(P, GSrc{lx0}, GMag{lom}, xi, __ldg(lom + t), walk, dv);
+    });
+    if (!any) return;
+    const uint32_t id = __ldg(lid + t);
+    float4 v = vel[id];
+    v.x += dv.x;
+    v.y += dv.y;
+    v.z += dv.z;
+    vel[id] = v;
+}
+
 // ---- launchers ------------------------------------------------------------------------------
 static inline unsigned dgrid(uint32_t n) { return (n + kDThreads - 1) / kDThreads; }
 static inline unsigned capped_grid(uint32_t n, uint32_t threads, int sms, uint32_t per_sm)
@@ -728,6 +754,18 @@ void launch_d_order(const DevParams& P, const DenseArgs& D, const float4* X, uin
     k_d_scan_sums<<<1, 1024, 0, st>>>(block_sums, nb);
     k_d_place<<<g, 256, 0, st>>>(P.n, slot_of, cnt, block_sums, order);
     *launches += 4;
+}
+
+void launch_d_order_recorded(const DevParams& P, const DenseArgs& D, const uint32_t* slot_of, uint32_t* cnt,
+                             uint32_t* block_sums, uint32_t* order, cudaStream_t st, uint64_t* launches)
+{
+    const uint32_t m = D.nx * D.ny * D.nz + 1u;
+    const uint32_t nb = order_scan_blocks(m - 1u);
+    const unsigned g = (P.n + 255u) / 256u;
+    k_d_scan_blocks<<<nb, 1024, 0, st>>>(cnt, m, block_sums);
+    k_d_scan_sums<<<1, 1024, 0, st>>>(block_sums, nb);
+    k_d_place<<<g, 256, 0, st>>>(P.n, slot_of, cnt, block_sums, order);
+    *launches += 3;
 }
 
 void launch_d_lambda(const DevParams& P, const DenseArgs& D, const float4* lx_in, float4* lx_out, float* lrho,

@@ -443,6 +443,8 @@ DenseArgs pbf_handle::dense_args() const
     D.hm = dhm;
     D.hcnt = dhcnt;
     D.use_list = 0;
+    D.rec_slot = nullptr;
+    D.rec_cnt = nullptr;
     D.clean = dclean;
     D.dcol = ddcol;
     D.dirty = ddirty;
@@ -612,9 +614,23 @@ int pbf_handle::stage(int st, uint32_t iter)
         // after the first iteration the particles have moved off their
         // predict-time cells: threads take them by current cell (lambda
         // computes the order, the delta-p of the same iteration reuses it)
+        // (a pass that moves particles records the slots of its outputs, so the
+        // order of the next pass needs only the scan and the placement)
         auto order_by = [&](const float4* X) {
-            launch_d_order(P, D, X, dslot, dcnt, dbsum, dord, stream, &launches);
+            if (dslot_fresh)
+                launch_d_order_recorded(P, D, dslot, dcnt, dbsum, dord, stream, &launches);
+            else
+                launch_d_order(P, D, X, dslot, dcnt, dbsum, dord, stream, &launches);
+            dslot_fresh = false;
             D.order = dord;
+        };
+        const size_t slots = (size_t)dwin_n[0] * dwin_n[1] * dwin_n[2];
+        auto record_next = [&]() -> int {
+            CK(cudaMemsetAsync(dcnt, 0, sizeof(uint32_t) * (slots + 1), stream));
+            D.rec_slot = dslot;
+            D.rec_cnt = dcnt;
+            dslot_fresh = true;
+            return PBF_OK;
         };
         switch (st) {
         case PBF_STAGE_LAMBDA:
@@ -630,6 +646,7 @@ int pbf_handle::stage(int st, uint32_t iter)
             if (iter >= 2 && dord_iter == (int)iter) D.order = dord;
             D.use_list = dlist_iter == (int)iter ? 1 : 0;
             dlist_iter = 0;
+            if (const int rc = record_next()) return rc;
             launch_d_deltap(P, D, lx[1], lx[0], stream);
             last_x = 0;
             break;
@@ -637,6 +654,9 @@ int pbf_handle::stage(int st, uint32_t iter)
             order_by(lx[0]);
             dord_iter = 0;
             dlist_iter = 0;
+            if (P.vort_on) {
+                if (const int rc = record_next()) return rc;
+            }
             launch_d_integrate(P, D, lx[0], lv, lx0, lom, lid, pos, vel, stream);
             break;
         default:
@@ -697,6 +717,7 @@ int pbf_handle::stage(int st, uint32_t iter)
             CK(cudaMemsetAsync(ddirty, 0, slots, stream));
             dord_iter = 0;
             dlist_iter = 0;
+            dslot_fresh = false;
             CK(cudaMemsetAsync(dflag, 0, sizeof(uint32_t), stream));
             label_space = true;
             last_x = 0;

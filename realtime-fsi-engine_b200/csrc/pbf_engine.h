@@ -74,6 +74,7 @@ struct pbf_handle {
     uint32_t *dslot = nullptr, *dord = nullptr, *dcnt = nullptr, *dbsum = nullptr;
     uint32_t cap_ord_n = 0;
     int dord_iter = 0;           // solver iteration the order was computed for (0: none)
+    bool dslot_fresh = false;    // dslot/dcnt hold the slots of the latest positions (recorded by a pass)
     // lambda hit masks replayed by the delta-p pass of the same iteration
     uint32_t* dhm = nullptr;
     uint8_t* dhcnt = nullptr;

@@ -136,6 +136,8 @@ struct DenseArgs {
     uint32_t* hm;          // lambda hit masks for the delta-p of the same iteration (kDenseListWords x n)
     uint8_t* hcnt;         // per label: chunks recorded, 0xFF = none
     int use_list;          // delta-p: the lambda pass of this iteration recorded hm/hcnt
+    uint32_t* rec_slot;    // delta-p / integrate (may be null): current slot of each output position
+    uint32_t* rec_cnt;     //   and per-slot counts (zeroed by the caller), for the next pass's order
     const uint8_t* clean;  // per window slot: 1 = no hash collision near the cell
     const uint8_t* dcol;   // per window slot: Chebyshev distance to the nearest other cell of its bucket
     uint8_t* dirty;        // per window slot: a moved particle with a colliding cell near is within reach
@@ -156,6 +158,9 @@ void launch_d_runs(const DenseArgs& D, const int2* cells, int2* runs, int sms, c
 uint32_t order_scan_blocks(uint32_t slots);
 void launch_d_order(const DevParams& P, const DenseArgs& D, const float4* X, uint32_t* slot_of, uint32_t* cnt,
                     uint32_t* block_sums, uint32_t* order, cudaStream_t st, uint64_t* launches);
+// The same order from slots and counts a pass recorded (DenseArgs::rec_slot / rec_cnt).
+void launch_d_order_recorded(const DevParams& P, const DenseArgs& D, const uint32_t* slot_of, uint32_t* cnt,
+                             uint32_t* block_sums, uint32_t* order, cudaStream_t st, uint64_t* launches);
 void launch_d_lambda(const DevParams& P, const DenseArgs& D, const float4* lx_in, float4* lx_out, float* lrho,
                      cudaStream_t st);
 void launch_d_deltap(const DevParams& P, const DenseArgs& D, const float4* lx_in, float4* lx_out, cudaStream_t st);
