@@ -187,6 +187,36 @@ __device__ __forceinline__ void masked_range(const float4* __restrict__ X, float
     }
 }
 
+// masked_range for candidates that are labels (a run): the query's own label
+// is cleared from each chunk's mask once instead of being compared with every
+// candidate.
+template <int C, class Hit, class Body, class Rec = NoRecord>
+__device__ __forceinline__ void label_range(const float4* __restrict__ X, float4 xi, int self, int lo, int hi,
+                                            Hit&& hit, Body&& body, Rec&& rec = Rec{})
+{
+    static_assert(C >= 1 && C <= 32, "hit mask is 32 bits");
+#pragma unroll 1
+    for (int k0 = lo; k0 < hi; k0 += C) {
+        uint32_t m = 0;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            const float4 xj = __ldg(X + k0 + c);
+            const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+            if (hit(rx * rx + ry * ry + rz * rz)) m |= 1u << c;
+        }
+        const uint32_t ds = (uint32_t)(self - k0);
+        if (ds < (uint32_t)C) m &= ~(1u << ds);
+        const int left = hi - k0;
+        if (left < C) m &= (1u << left) - 1u;
+        rec(m);
+        while (m) {
+            const int c = __ffs(m) - 1;
+            m &= m - 1u;
+            body(k0 + c);
+        }
+    }
+}
+
 struct IdMap {
     __device__ __forceinline__ int operator()(int k) const { return k; }
 };
@@ -197,6 +227,7 @@ struct InvMap {
 
 // Candidates per hit mask in a run (a run holds about 24).
 constexpr int kRunChunk = 16;
+static_assert(kRunChunk <= kLabelPad, "a run's last chunk stays inside the padded label arrays");
 
 // The 9 x-runs of a particle whose cell satisfies (a), (b) and (c).
 struct RunWalk {
@@ -214,7 +245,7 @@ struct RunWalk {
 #pragma unroll 1
             for (int dy = -1; dy <= 1; ++dy) {
                 const int2 r = __ldg(runs + s0 + dz * nxy + dy * nx);
-                masked_range<kRunChunk>(X, xi, self, r.x, r.y, IdMap{}, hit, body);
+                label_range<kRunChunk>(X, xi, self, r.x, r.y, hit, body);
             }
         }
     }
@@ -252,7 +283,7 @@ struct RunWalkRec {
 #pragma unroll 1
             for (int dy = -1; dy <= 1; ++dy) {
                 const int2 r = __ldg(runs + s0 + dz * nxy + dy * nx);
-                masked_range<kRunChunk>(X, xi, self, r.x, r.y, IdMap{}, hit, body, [&](uint32_t m) {
+                label_range<kRunChunk>(X, xi, self, r.x, r.y, hit, body, [&](uint32_t m) {
                     if (q < kListChunks) {
                         if (q & 1)
                             hm[(size_t)(q >> 1) * n + self] = word | (m << 16);

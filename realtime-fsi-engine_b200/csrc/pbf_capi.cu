@@ -400,9 +400,10 @@ int pbf_handle::ensure_label_capacity()
 {
     int rc;
     if (cap_label_n < n || !inv) {
-        const size_t c = std::max<uint32_t>(n, 1u);
-        if ((rc = dalloc(lx[0], c)) || (rc = dalloc(lx[1], c)) || (rc = dalloc(lxb, c)) || (rc = dalloc(lv, c)) ||
-            (rc = dalloc(lx0, c)) || (rc = dalloc(lom, c)) || (rc = dalloc(lrho, c)) || (rc = dalloc(lid, c)) ||
+        // (kLabelPad entries past the last label: a run's last chunk loads them and masks them out)
+        const size_t c = std::max<uint32_t>(n, 1u), cp = c + kLabelPad;
+        if ((rc = dalloc(lx[0], cp)) || (rc = dalloc(lx[1], cp)) || (rc = dalloc(lxb, c)) || (rc = dalloc(lv, cp)) ||
+            (rc = dalloc(lx0, cp)) || (rc = dalloc(lom, cp)) || (rc = dalloc(lrho, c)) || (rc = dalloc(lid, c)) ||
             (rc = dalloc(lkey, c)) || (rc = dalloc(inv, c)))
             return rc;
         cap_label_n = (uint32_t)c;

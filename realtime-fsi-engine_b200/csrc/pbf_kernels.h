@@ -129,6 +129,9 @@ void launch_l_unpermute1(uint32_t n, const uint32_t* inv, const float* src, floa
 
 // ---- k_dense.cu: x-runs of a dense cell window over relabelled data ----------
 constexpr int kDenseListWords = 16;
+// Label-space position/velocity arrays hold this many entries past the last
+// label, so a run's last chunk of candidates may load past the run's end.
+constexpr int kLabelPad = 32;
 struct DenseArgs {
     const int2* table;     // per window slot: label range of its particles, (-1, -1) when empty
     const int2* runs;      // per window slot: label range of slots s-1 .. s+1 of its row
