@@ -195,20 +195,28 @@ __device__ __forceinline__ void label_range(const float4* __restrict__ X, float4
                                             Hit&& hit, Body&& body, Rec&& rec = Rec{})
 {
     static_assert(C >= 1 && C <= 32, "hit mask is 32 bits");
+    constexpr int G = 32 / C;  // chunks tested before one drain of up to 32 candidates
 #pragma unroll 1
-    for (int k0 = lo; k0 < hi; k0 += C) {
+    for (int k0 = lo; k0 < hi; k0 += G * C) {
         uint32_t m = 0;
+#pragma unroll 1
+        for (int g = 0; g < G; ++g) {
+            const int kb = k0 + g * C;
+            if (kb >= hi) break;
+            uint32_t mg = 0;
 #pragma unroll
-        for (int c = 0; c < C; ++c) {
-            const float4 xj = __ldg(X + k0 + c);
-            const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-            if (hit(rx * rx + ry * ry + rz * rz)) m |= 1u << c;
+            for (int c = 0; c < C; ++c) {
+                const float4 xj = __ldg(X + kb + c);
+                const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+                if (hit(rx * rx + ry * ry + rz * rz)) mg |= 1u << c;
+            }
+            const uint32_t ds = (uint32_t)(self - kb);
+            if (ds < (uint32_t)C) mg &= ~(1u << ds);
+            const int left = hi - kb;
+            if (left < C) mg &= (1u << left) - 1u;
+            rec(mg);
+            m |= mg << (g * C);
         }
-        const uint32_t ds = (uint32_t)(self - k0);
-        if (ds < (uint32_t)C) m &= ~(1u << ds);
-        const int left = hi - k0;
-        if (left < C) m &= (1u << left) - 1u;
-        rec(m);
         while (m) {
             const int c = __ffs(m) - 1;
             m &= m - 1u;
@@ -721,7 +729,7 @@ __global__ void __launch_bounds__(kDThreads, 10) k_d_integrate(DevParams P, Dens
     if (D.rec_cnt) record_slot(P, D, xo, t, live);
 }
 
-__global__ void __launch_bounds__(kDThreads) k_d_vorticity(DevParams P, DenseArgs D, const float4* __restrict__ lx0,
+__global__ void __launch_bounds__(kDThreads, 12) k_d_vorticity(DevParams P, DenseArgs D, const float4* __restrict__ lx0,
                                                            const float4* __restrict__ lom,
                                                            const uint32_t* __restrict__ lid, float4* __restrict__ vel)
 {
