@@ -96,6 +96,7 @@ __device__ __forceinline__ bool project_vjp(const SdfDev& S, float3 x, float3& x
     if (sdf_far_obstacle(S, x.x, x.y, x.z)) return false;
     const float e = S.cell;
     const float d = sdf_sample(S, x.x, x.y, x.z);
+    if (S.containment ? !(d > -S.padding) : !(d < S.padding)) return false;  // no contact
     const float inv2e = 1.0f / (2.0f * e);
     const float gx = (sdf_sample(S, x.x + e, x.y, x.z) - sdf_sample(S, x.x - e, x.y, x.z)) * inv2e;
     const float gy = (sdf_sample(S, x.x, x.y + e, x.z) - sdf_sample(S, x.x, x.y - e, x.z)) * inv2e;

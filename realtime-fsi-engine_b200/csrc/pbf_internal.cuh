@@ -194,6 +194,8 @@ __device__ __forceinline__ bool sdf_project(const SdfDev& S, float3& p, float3& 
     if (sdf_far_obstacle(S, p.x, p.y, p.z)) return false;
     const float e = S.cell;
     const float d = sdf_sample(S, p.x, p.y, p.z);
+    // no contact whatever the gradient: skip its six samples
+    if (S.containment ? !(d > -S.padding) : !(d < S.padding)) return false;
     const float inv2e = 1.0f / (2.0f * e);
     const float gx = (sdf_sample(S, p.x + e, p.y, p.z) - sdf_sample(S, p.x - e, p.y, p.z)) * inv2e;
     const float gy = (sdf_sample(S, p.x, p.y + e, p.z) - sdf_sample(S, p.x, p.y - e, p.z)) * inv2e;
