@@ -62,20 +62,21 @@ __device__ __forceinline__ float box_d2(float3 p, float4 lo, float4 hi)
     return d2;
 }
 
-// Branch-and-bound nearest face, nearer child first (TriangleBVH::query,
-// SDFBoundary.cpp:225-257, as an explicit stack).
-__device__ Hit mesh_closest(const MeshDev& M, float3 P)
+// Branch-and-bound nearest face of the subtree at `root`, nearer child first
+// (TriangleBVH::query, SDFBoundary.cpp:225-257, as an explicit stack); the
+// first face met with the smallest squared distance wins.
+__device__ Hit subtree_closest(const MeshDev& M, float3 P, int root, float bound = 3.0e38f)
 {
     Hit best;
-    best.d2 = 3.0e38f;
+    best.d2 = bound;
     best.p = make_float3(0.f, 0.f, 0.f);
     best.feature = 0;
     best.face = -1;
-    if (M.nf <= 0) return best;
+    if (M.nf <= 0 || root < 0) return best;
     const int n_int = M.nf - 1;
     int stack[64];
     int sp = 0;
-    stack[sp++] = 0;
+    stack[sp++] = root;
     while (sp > 0) {
         const int node = stack[--sp];
         if (box_d2(P, __ldg(M.bmin + node), __ldg(M.bmax + node)) >= best.d2) continue;
@@ -105,6 +106,56 @@ __device__ Hit mesh_closest(const MeshDev& M, float3 P)
         if (dnear < best.d2 && sp < 64) stack[sp++] = nearc;
     }
     return best;
+}
+
+__device__ Hit mesh_closest(const MeshDev& M, float3 P) { return subtree_closest(M, P, 0); }
+
+__device__ __forceinline__ float centre_d2(float3 p, float4 lo, float4 hi)
+{
+    const float x = 0.5f * (lo.x + hi.x) - p.x, y = 0.5f * (lo.y + hi.y) - p.y, z = 0.5f * (lo.z + hi.z) - p.z;
+    return x * x + y * y + z * z;
+}
+
+// Squared distance to the face reached by taking the nearer child from
+// `root` (by box distance, then by box centre when P lies in both boxes, as
+// it does inside a closed mesh): an upper bound of the subtree's nearest
+// distance.
+__device__ float first_leaf_d2(const MeshDev& M, float3 P, int root)
+{
+    const int n_int = M.nf - 1;
+    int node = root;
+    while (node < n_int) {
+        const int2 ch = __ldg(M.child + node);
+        const float4 l0 = __ldg(M.bmin + ch.x), l1 = __ldg(M.bmax + ch.x);
+        const float4 r0 = __ldg(M.bmin + ch.y), r1 = __ldg(M.bmax + ch.y);
+        const float dl = box_d2(P, l0, l1), dr = box_d2(P, r0, r1);
+        const bool left = dl != dr ? dl < dr : centre_d2(P, l0, l1) <= centre_d2(P, r0, r1);
+        node = left ? ch.x : ch.y;
+    }
+    const int f = __ldg(M.leaf_face + (node - n_int));
+    const int3 tri = M.faces[f];
+    int feat;
+    const float3 cp = closest_on_triangle(P, M.verts[tri.x], M.verts[tri.y], M.verts[tri.z], feat);
+    const float3 dd = f3sub(P, cp);
+    return f3dot(dd, dd);
+}
+
+// Position of the subtree at `node` in mesh_closest's visiting order for the
+// point P: the near (0) / far (1) choices on the path from the root, root
+// first, as the high bits of a key.  Disjoint subtrees compare as their
+// first-visited faces do.
+__device__ uint32_t visit_rank(const MeshDev& M, float3 P, int node)
+{
+    uint32_t bits = 0;
+    int len = 0;
+    for (int c = node, p = M.parent[node]; p >= 0 && len < 32; c = p, p = M.parent[p], ++len) {
+        const int2 ch = __ldg(M.child + p);
+        const float dl = box_d2(P, __ldg(M.bmin + ch.x), __ldg(M.bmax + ch.x));
+        const float dr = box_d2(P, __ldg(M.bmin + ch.y), __ldg(M.bmax + ch.y));
+        const int nearc = dl <= dr ? ch.x : ch.y;
+        bits |= (c == nearc ? 0u : 1u) << len;
+    }
+    return len ? bits << (32 - len) : 0u;
 }
 
 // ---- LBVH construction ------------------------------------------------------------
@@ -220,23 +271,45 @@ __device__ __forceinline__ float3 pseudo_normal(const MeshDev& M, const Hit& h)
     }
 }
 
-__global__ void k_mesh_grid(MeshDev M, int dx, int dy, int dz, double ox, double oy, double oz, double cell,
-                            float* __restrict__ out)
+// One warp per voxel: lane l searches the subtree at M.frontier[l] (the
+// frontier covers the tree) for faces within the warp's bound U, then the
+// warp keeps the smallest squared distance and, among equal ones, the
+// subtree mesh_closest would visit first.  Within a subtree the search is mesh_closest's, so the winner is the
+// face, point and feature a single mesh_closest walk returns; the walk's
+// length is split over 32 lanes (a voxel deep inside a closed mesh has almost
+// every face within its bound).
+__global__ void __launch_bounds__(128) k_mesh_grid(MeshDev M, int dx, int dy, int dz, double ox, double oy,
+                                                   double oz, double cell, float* __restrict__ out)
 {
     const long total = (long)dx * dy * dz;
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const long warps = (long)gridDim.x * (blockDim.x >> 5);
+    const int root = M.frontier[lane];
+    for (long i = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
         const int z = (int)(i % dz);
         const int y = (int)((i / dz) % dy);
         const int x = (int)(i / ((long)dy * dz));
         const float3 P = make_float3((float)(ox + x * cell), (float)(oy + y * cell), (float)(oz + z * cell));
-        const Hit h = mesh_closest(M, P);
-        float d = 0.0f;
-        if (h.face >= 0) {
-            const float3 pn = pseudo_normal(M, h);
-            const float s = (f3dot(f3sub(P, h.p), pn) >= 0.0f) ? 1.0f : -1.0f;
-            d = s * sqrtf(h.d2);
+        // U: the smallest first-leaf distance over the lanes, reached by some
+        // face, so the nearest distance is <= U; a lane then searches only for
+        // faces within U (the bound just above U keeps faces at exactly U)
+        const uint32_t ub = __reduce_min_sync(0xFFFFFFFFu,
+                                              root >= 0 ? __float_as_uint(first_leaf_d2(M, P, root)) : 0x7F7FFFFFu);
+        const Hit h = subtree_closest(M, P, root, nextafterf(__uint_as_float(ub), 3.0e38f));
+        const uint32_t d2b = __float_as_uint(h.d2);  // non-negative: bit order = value order
+        const uint32_t rank = root >= 0 ? visit_rank(M, P, root) : 0xFFFFFFFFu;
+        const uint32_t dmin = __reduce_min_sync(0xFFFFFFFFu, d2b);
+        const uint32_t rmin = __reduce_min_sync(0xFFFFFFFFu, d2b == dmin ? rank : 0xFFFFFFFFu);
+        const uint32_t win = __ballot_sync(0xFFFFFFFFu, d2b == dmin && rank == rmin);
+        if (lane == __ffs(win) - 1) {
+            float d = 0.0f;
+            if (h.face >= 0) {
+                const float3 pn = pseudo_normal(M, h);
+                const float s = (f3dot(f3sub(P, h.p), pn) >= 0.0f) ? 1.0f : -1.0f;
+                d = s * sqrtf(h.d2);
+            }
+            out[i] = d;
         }
-        out[i] = d;
     }
 }
 
@@ -244,7 +317,7 @@ void launch_mesh_grid_d(MeshDev M, int dx, int dy, int dz, const double* o, doub
                         cudaStream_t st)
 {
     const long total = (long)dx * dy * dz;
-    long blocks = (total + 127) / 128;
+    long blocks = (total + 3) / 4;  // four voxels (warps) per block
     if (blocks > (long)sms * 16) blocks = (long)sms * 16;
     if (blocks < 1) blocks = 1;
     k_mesh_grid<<<(unsigned)blocks, 128, 0, st>>>(M, dx, dy, dz, o[0], o[1], o[2], cell, out);

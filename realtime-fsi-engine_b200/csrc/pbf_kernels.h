@@ -205,7 +205,9 @@ struct MeshDev {
     float4* bmax;         // 2nf-1
     int* leaf_face;       // nf: face index of leaf i (Morton order)
     uint32_t* flags;      // nf-1 refit arrival counters
+    const int* frontier;  // kMeshFrontier subtree roots that together cover the tree (-1: unused)
 };
+constexpr int kMeshFrontier = 32;  // one per lane of the grid kernel's warp
 void launch_mesh_refit(MeshDev M, cudaStream_t st, uint64_t* launches);
 void launch_mesh_grid_d(MeshDev M, int dx, int dy, int dz, const double* origin, double cell, float* out, int sms,
                         cudaStream_t st);

@@ -48,6 +48,7 @@ struct MeshHost {
     uint32_t* d_flags = nullptr;
     uint32_t *d_codes = nullptr, *d_ka = nullptr, *d_ia = nullptr, *d_kb = nullptr, *d_ib = nullptr;
     uint32_t *d_hist = nullptr, *d_tot = nullptr;
+    int* d_frontier = nullptr;
 };
 
 struct D3 {
@@ -86,8 +87,44 @@ void free_mesh_host(MeshHost* m)
     dfree(m->d_faces); dfree(m->d_verts); dfree(m->d_face_n); dfree(m->d_edge_n); dfree(m->d_vert_n);
     dfree(m->d_child); dfree(m->d_parent); dfree(m->d_bmin); dfree(m->d_bmax); dfree(m->d_leaf_face);
     dfree(m->d_flags); dfree(m->d_codes); dfree(m->d_ka); dfree(m->d_ia); dfree(m->d_kb); dfree(m->d_ib);
-    dfree(m->d_hist); dfree(m->d_tot);
+    dfree(m->d_hist); dfree(m->d_tot); dfree(m->d_frontier);
     delete m;
+}
+
+// kMeshFrontier subtrees that together cover the tree (internal nodes [0,
+// nf-1), leaves [nf-1, 2nf-1)): starting from the root, the internal node
+// with the most leaves is replaced by its two children until there are
+// kMeshFrontier subtrees or only leaves; unused entries are -1.
+std::vector<int> mesh_frontier(const std::vector<int2>& child, int nf)
+{
+    std::vector<int> fr(kMeshFrontier, -1);
+    const int n_int = nf - 1;
+    fr[0] = 0;
+    if (n_int <= 0) return fr;
+    const int nodes = 2 * nf - 1;
+    std::vector<int> leaves(n_int, 0), order;
+    order.reserve(n_int);
+    std::vector<int> st{0};
+    while (!st.empty() && (int)order.size() < n_int) {
+        const int u = st.back();
+        st.pop_back();
+        order.push_back(u);
+        for (const int c : {child[u].x, child[u].y})
+            if (c >= 0 && c < n_int) st.push_back(c);
+    }
+    auto count = [&](int c) { return c >= n_int && c < nodes ? 1 : (c >= 0 && c < n_int ? leaves[c] : 0); };
+    for (auto it = order.rbegin(); it != order.rend(); ++it) leaves[*it] = count(child[*it].x) + count(child[*it].y);
+    int used = 1;
+    while (used < kMeshFrontier) {
+        int j = -1;
+        for (int k = 0; k < used; ++k)
+            if (fr[k] < n_int && (j < 0 || leaves[fr[k]] > leaves[fr[j]])) j = k;
+        if (j < 0) break;
+        const int2 ch = child[fr[j]];
+        fr[j] = ch.x;
+        fr[used++] = ch.y;
+    }
+    return fr;
 }
 
 }  // namespace
@@ -245,6 +282,20 @@ extern "C" int pbf_set_sdf_mesh(pbf_handle* h, const double* verts, int32_t nv, 
     CK(cudaMemcpyAsync(m->d_leaf_face, sid, sizeof(int) * nf, cudaMemcpyDeviceToDevice, st));
     launch_lbvh_topology(nf, sk, m->d_child, m->d_parent, st);
     h->launches += 2;
+    {
+        // the grid kernel's per-lane subtrees (the topology is fixed until the next build)
+        std::vector<int2> child(std::max(1, nf - 1), make_int2(-1, -1));
+        if (nf > 1)
+            CK(cudaMemcpyAsync(child.data(), m->d_child, sizeof(int2) * (size_t)(nf - 1), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        const std::vector<int> fr = mesh_frontier(child, nf);
+        if ((rc = dalloc(m->d_frontier, (size_t)kMeshFrontier))) {
+            h->mesh_free();
+            return rc;
+        }
+        CK(cudaMemcpyAsync(m->d_frontier, fr.data(), sizeof(int) * kMeshFrontier, cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+    }
 
     MeshDev M{};
     M.nv = nv;
@@ -260,6 +311,7 @@ extern "C" int pbf_set_sdf_mesh(pbf_handle* h, const double* verts, int32_t nv, 
     M.bmax = m->d_bmax;
     M.leaf_face = m->d_leaf_face;
     M.flags = m->d_flags;
+    M.frontier = m->d_frontier;
     h->mesh = M;
     launch_mesh_refit(M, st, &h->launches);
 

@@ -77,6 +77,29 @@ def test_refit_after_deformation_matches_oracle(have_gpu):
         O.lib().orc_mesh_free(m)
 
 
+def test_grid_is_the_single_walk_distance(have_gpu):
+    """The grid kernel splits each voxel's nearest-face search over 32 subtrees
+    of the LBVH; every voxel's |distance| is the one the single-walk
+    closest-triangle query finds at the voxel centre, before and after a
+    refit of a deformed mesh (no longer symmetric)."""
+    for subdiv, cell in [(1, 0.05), (4, 0.0125)]:
+        V, F = scenes.icosphere(subdiv, 0.2, (0.8, 0.3, 0.5))
+        sdf = P.SDFBoundary()
+        sdf.buildFromMesh(V, F, cell)
+        rng = np.random.default_rng(subdiv)
+        for verts in (None, V + rng.normal(0, 0.003, V.shape)):
+            if verts is not None:
+                sdf.refitFromMesh(verts)
+            dims, org = sdf.dimensions(), sdf.origin()
+            idx = np.indices(dims).reshape(3, -1).T
+            pts = (org + idx * cell).astype(np.float32)
+            _, point = sdf.closest_many(pts)
+            walk = np.sqrt(((point.astype(np.float64) - pts) ** 2).sum(1))
+            g = sdf.distances()
+            assert np.abs(np.abs(g) - walk).max() < 2e-7
+            assert (g < 0).sum() > 0 and (g > 0).sum() > 0
+
+
 def test_closest_triangle_matches_oracle(have_gpu):
     V, F = scenes.icosphere(3, 0.2, (0.8, 0.3, 0.5))
     sdf = P.SDFBoundary()
