@@ -397,11 +397,19 @@ int pbf_batch_kernel_launches(const pbf_batch* b, uint64_t* count);
  *                           Morton order of their cells; 0: sorted (hash) order
  *   PBF_BOPT_BLOCKS_PER_SM  persistent grid of SMs x value blocks looping over the
  *                           particles; 0 (default): one thread per particle
- *   PBF_BOPT_USE_GRAPH      1 (default): replay the step from a CUDA graph */
+ *   PBF_BOPT_USE_GRAPH      1 (default): replay the step from a CUDA graph
+ *   PBF_BOPT_NEIGHBOUR_MODE -1 (default): automatic (the autotuner's pick once it has run,
+ *                           before that 8 from 2^19 particles when the windows fit, else 4);
+ *                           4: every scene walks its 27 hashed buckets (block, order and
+ *                           persistence apply); 8: a dense cell window per scene (the walls'
+ *                           box plus 6 cells each side, at most 2^26 cells in all, APBF off),
+ *                           the passes of PBF_OPT_SPATIAL_ORDER mode 8 over all scenes at once.
+ *                           Both give every scene the bits of its own pbf_handle. */
 #define PBF_BOPT_BLOCK 1
 #define PBF_BOPT_ORDER 2
 #define PBF_BOPT_BLOCKS_PER_SM 3
 #define PBF_BOPT_USE_GRAPH 4
+#define PBF_BOPT_NEIGHBOUR_MODE 5
 int pbf_batch_set_option(pbf_batch* b, int option, int value);
 int pbf_batch_get_option(const pbf_batch* b, int option, int* value);
 
@@ -410,10 +418,13 @@ typedef struct pbf_batch_tuning {
     int32_t order;
     int32_t blocks_per_sm;
     float ms_per_step;
+    int32_t neighbour_mode;  /* 4 or 8 (block, order and persistence apply to 4 only) */
 } pbf_batch_tuning;
-/* Times every candidate (block x order x persistence) for `trial_steps` steps
- * after one warm-up step, keeps the fastest and restores the particle state
- * that the trials advanced.  `results` (may be null) receives up to
+/* Times every candidate for `trial_steps` steps after one warm-up step, keeps
+ * the fastest and restores the particle state that the trials advanced.  The
+ * candidates: block x order x persistence in neighbour mode 4, and mode 8 when
+ * the windows fit, as PBF_BOPT_NEIGHBOUR_MODE allows (-1: both; the pick then
+ * decides the automatic mode).  `results` (may be null) receives up to
  * `max_results` timed candidates, `*num_results` their count; `*best` the pick. */
 int pbf_batch_autotune(pbf_batch* b, uint32_t trial_steps, pbf_batch_tuning* best, pbf_batch_tuning* results,
                        uint32_t max_results, uint32_t* num_results);

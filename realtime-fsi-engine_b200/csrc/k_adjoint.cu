@@ -136,25 +136,6 @@ __device__ __forceinline__ bool project_vjp(const SdfDev& S, float3 x, float3& x
     return true;
 }
 
-__device__ __forceinline__ SdfDev ad_load_sdf(const SceneDev* S)
-{
-    SdfDev d;
-    d.enabled = __ldg(&S->sdf.enabled);
-    d.dist = S->sdf.dist;
-    d.slab_min = S->sdf.slab_min;
-    d.dx = __ldg(&S->sdf.dx);
-    d.dy = __ldg(&S->sdf.dy);
-    d.dz = __ldg(&S->sdf.dz);
-    d.ox = __ldg(&S->sdf.ox);
-    d.oy = __ldg(&S->sdf.oy);
-    d.oz = __ldg(&S->sdf.oz);
-    d.cell = __ldg(&S->sdf.cell);
-    d.inv_cell = __ldg(&S->sdf.inv_cell);
-    d.padding = __ldg(&S->sdf.padding);
-    d.containment = __ldg(&S->sdf.containment);
-    return d;
-}
-
 __device__ __forceinline__ void add_t(float* tgrad, int k, float3 tb)
 {
     if (tb.x != 0.0f) atomicAdd(tgrad + 4 * k + 0, tb.x);
@@ -195,7 +176,7 @@ __global__ void __launch_bounds__(kAThreads) k_ad_deltap_rec(DevParams P, const 
                                                              float4* __restrict__ auxd)
 {
     AD_PROLOGUE
-    const SdfDev sdf = ad_load_sdf(SC);
+    const SdfDev sdf = load_sdf(SC);
     float3 dp;
     xout[s] = deltap_particle_x(P, tab, mask, sdf, xl, s, dp);
     auxd[s] = make_float4(dp.x, dp.y, dp.z, 0.0f);
@@ -273,7 +254,7 @@ __global__ void __launch_bounds__(kAThreads) k_ad_integrate(
     float4* __restrict__ gv, float4* __restrict__ x0b, float* __restrict__ tgrad)
 {
     AD_PROLOGUE
-    const SdfDev sdf = ad_load_sdf(SC);
+    const SdfDev sdf = load_sdf(SC);
     const float4 x4 = __ldg(xs + s);
     const float4 v0 = __ldg(sv + s);
     const uint32_t id = __ldg(ids + s);
@@ -438,7 +419,7 @@ __global__ void __launch_bounds__(kAThreads) k_ad_deltap(DevParams P, const Scen
     }
     const float3 x = make_float3(xi.x + dx, xi.y + dy, xi.z + dz);
     float3 xb = make_float3(g4.x, g4.y, g4.z);
-    const SdfDev sdf = ad_load_sdf(SC);
+    const SdfDev sdf = load_sdf(SC);
     if (sdf.enabled) {
         float3 tb = make_float3(0.f, 0.f, 0.f);
         project_vjp(sdf, x, xb, make_float3(0.f, 0.f, 0.f), tb);

@@ -110,25 +110,6 @@ __global__ void __launch_bounds__(B) k_b_lambda(DevParams P, const SceneDev* __r
     }
 }
 
-__device__ __forceinline__ SdfDev load_sdf(const SceneDev* S)
-{
-    SdfDev d;
-    d.enabled = __ldg(&S->sdf.enabled);
-    d.dist = S->sdf.dist;
-    d.slab_min = S->sdf.slab_min;
-    d.dx = __ldg(&S->sdf.dx);
-    d.dy = __ldg(&S->sdf.dy);
-    d.dz = __ldg(&S->sdf.dz);
-    d.ox = __ldg(&S->sdf.ox);
-    d.oy = __ldg(&S->sdf.oy);
-    d.oz = __ldg(&S->sdf.oz);
-    d.cell = __ldg(&S->sdf.cell);
-    d.inv_cell = __ldg(&S->sdf.inv_cell);
-    d.padding = __ldg(&S->sdf.padding);
-    d.containment = __ldg(&S->sdf.containment);
-    return d;
-}
-
 template <int B>
 __global__ void __launch_bounds__(B) k_b_deltap(DevParams P, const SceneDev* __restrict__ scenes,
                                                 const uint16_t* __restrict__ scene_of, const float4* __restrict__ xin,

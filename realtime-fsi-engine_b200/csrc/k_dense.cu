@@ -41,11 +41,59 @@
 // into a hit mask exactly as the hashed-bucket passes do, so a pair's
 // arithmetic is the same in every walk.
 #include "masked_body.cuh"
+#include "pbf_batch.h"
 #include "pbf_kernels.h"
 
 namespace pbf {
 
 constexpr int kDThreads = 128;
+
+// Batches (B = true): the scene k of a label, hash-sorted index or slot
+// replaces the hash mask, walls, SDF and window of P and D with its own, so
+// the code below serves one scene and many alike.
+template <bool B>
+__device__ __forceinline__ void scene_view(DevParams& P, DenseArgs& D, uint32_t k)
+{
+    if constexpr (B) {
+        const SceneDev* S = D.scenes + k;
+        P.mask = __ldg(&S->mask);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            P.bmin[a] = __ldg(&S->bmin[a]);
+            P.bmax[a] = __ldg(&S->bmax[a]);
+        }
+        P.sdf = load_sdf(S);
+        D.gx0 = __ldg(&S->win_g0[0]);
+        D.gy0 = __ldg(&S->win_g0[1]);
+        D.gz0 = __ldg(&S->win_g0[2]);
+        D.nx = __ldg(&S->win_n[0]);
+        D.ny = __ldg(&S->win_n[1]);
+        D.nz = __ldg(&S->win_n[2]);
+        D.slot0 = __ldg(&S->slot0);
+        D.htable += __ldg(&S->table_off);
+    }
+}
+
+template <bool B>
+__device__ __forceinline__ void scene_of_label(DevParams& P, DenseArgs& D, int t)
+{
+    if constexpr (B) scene_view<B>(P, D, __ldg(D.scene_of + t));
+}
+
+// f(P, D) with the constants of label t's scene: the kernel's own for one
+// scene (B = false, read in place), a patched copy for a batch.
+template <bool B, class F>
+__device__ __forceinline__ void with_scene(const DevParams& P0, const DenseArgs& D0, int t, F&& f)
+{
+    if constexpr (B) {
+        DevParams P = P0;
+        DenseArgs D = D0;
+        scene_of_label<B>(P, D, t);
+        f(P, D);
+    } else {
+        f(P0, D0);
+    }
+}
 
 __device__ __forceinline__ uint32_t wrap_axis(int c, int g0, uint32_t n)
 {
@@ -58,27 +106,52 @@ __device__ __forceinline__ uint32_t wrap_axis(int c, int g0, uint32_t n)
 
 __device__ __forceinline__ uint32_t dense_key(const DenseArgs& D, int cx, int cy, int cz)
 {
-    return (wrap_axis(cz, D.gz0, D.nz) * D.ny + wrap_axis(cy, D.gy0, D.ny)) * D.nx + wrap_axis(cx, D.gx0, D.nx);
+    return D.slot0 +
+           (wrap_axis(cz, D.gz0, D.nz) * D.ny + wrap_axis(cy, D.gy0, D.ny)) * D.nx + wrap_axis(cx, D.gx0, D.nx);
 }
 
 // Window slot of each hash-sorted particle's predict-time cell.
-__global__ void __launch_bounds__(256) k_d_keys(DevParams P, DenseArgs D, const float4* __restrict__ sx,
+template <bool B>
+__global__ void __launch_bounds__(256) k_d_keys(DevParams P0, DenseArgs D0, const float4* __restrict__ sx,
                                                 uint32_t* __restrict__ dkey)
 {
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < P.n; s += stride) {
-        const float4 x = __ldg(sx + s);
-        dkey[s] = dense_key(D, cell_coord(x.x, P.h), cell_coord(x.y, P.h), cell_coord(x.z, P.h));
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < P0.n; s += stride) {
+        with_scene<B>(P0, D0, (int)s, [&](const DevParams& P, const DenseArgs& D) {
+            const float4 x = __ldg(sx + s);
+            dkey[s] = dense_key(D, cell_coord(x.x, P.h), cell_coord(x.y, P.h), cell_coord(x.z, P.h));
+        });
     }
 }
 
+// The window of global slot g (its scene's, in a batch) and g's slot in it.
+template <bool B>
+__device__ __forceinline__ uint32_t window_of_slot(DenseArgs& D, uint32_t& mask, uint32_t g)
+{
+    if constexpr (B) {
+        const SceneDev* S = D.scenes + __ldg(D.slot_scene + g);
+        mask = __ldg(&S->mask);
+        D.gx0 = __ldg(&S->win_g0[0]);
+        D.gy0 = __ldg(&S->win_g0[1]);
+        D.gz0 = __ldg(&S->win_g0[2]);
+        D.nx = __ldg(&S->win_n[0]);
+        D.ny = __ldg(&S->win_n[1]);
+        D.nz = __ldg(&S->win_n[2]);
+        D.slot0 = __ldg(&S->slot0);
+    }
+    return g - D.slot0;
+}
+
 // Conditions (a) and (b) per window slot.
-__global__ void __launch_bounds__(128) k_d_clean(DenseArgs D, uint32_t mask, uint8_t* __restrict__ clean,
+template <bool B>
+__global__ void __launch_bounds__(128) k_d_clean(DenseArgs D0, uint32_t mask0, uint8_t* __restrict__ clean,
                                                  uint32_t* __restrict__ unclean)
 {
-    const uint32_t slots = D.nx * D.ny * D.nz;
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += stride) {
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < D0.total; g += stride) {
+        DenseArgs D = D0;
+        uint32_t mask = mask0;
+        const uint32_t s = window_of_slot<B>(D, mask, g);
         const uint32_t lx = s % D.nx, ly = (s / D.nx) % D.ny, lz = s / (D.nx * D.ny);
         uint8_t ok = 0;
         if (lx >= 1 && lx + 1 < D.nx && ly >= 1 && ly + 1 < D.ny && lz >= 1 && lz + 1 < D.nz) {
@@ -100,38 +173,43 @@ __global__ void __launch_bounds__(128) k_d_clean(DenseArgs D, uint32_t mask, uin
             ok = good ? 1 : 0;
             if (!good) atomicAdd(unclean, 1u);
         }
-        clean[s] = ok;
+        clean[g] = ok;
     }
 }
 
 // Label range of the x-run centred on each window slot: slots s - 1, s, s + 1
 // of one row, (-1, -1) entries being empty cells; (0, 0) when all three are
 // empty and at the row ends (never walked: a walked cell is interior).
-__global__ void __launch_bounds__(256) k_d_runs(DenseArgs D, const int2* __restrict__ cells, int2* __restrict__ runs)
+template <bool B>
+__global__ void __launch_bounds__(256) k_d_runs(DenseArgs D0, const int2* __restrict__ cells, int2* __restrict__ runs)
 {
-    const uint32_t slots = D.nx * D.ny * D.nz;
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += stride) {
-        const uint32_t ux = s % D.nx;
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < D0.total; g += stride) {
+        DenseArgs D = D0;
+        uint32_t mask = 0;
+        const uint32_t ux = window_of_slot<B>(D, mask, g) % D.nx;
         int2 r = make_int2(0, 0);
         if (ux >= 1 && ux + 1 < D.nx) {
-            const int2 e0 = __ldg(cells + s - 1), e1 = __ldg(cells + s), e2 = __ldg(cells + s + 1);
+            const int2 e0 = __ldg(cells + g - 1), e1 = __ldg(cells + g), e2 = __ldg(cells + g + 1);
             const int hi = max(max(e0.y, e1.y), e2.y);
             // as unsigned, an empty cell's start (-1) is the largest
             if (hi >= 0) r = make_int2((int)min(min((uint32_t)e0.x, (uint32_t)e1.x), (uint32_t)e2.x), hi);
         }
-        runs[s] = r;
+        runs[g] = r;
     }
 }
 
 // Chebyshev distance from each window cell to the nearest other cell in the
 // same hash bucket, searched up to kDcolReach (kDcolReach + 1: none that near).
 constexpr int kDcolReach = 6;
-__global__ void __launch_bounds__(128) k_d_dcol(DenseArgs D, uint32_t mask, uint8_t* __restrict__ dcol)
+template <bool B>
+__global__ void __launch_bounds__(128) k_d_dcol(DenseArgs D0, uint32_t mask0, uint8_t* __restrict__ dcol)
 {
-    const uint32_t slots = D.nx * D.ny * D.nz;
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += stride) {
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < D0.total; g += stride) {
+        DenseArgs D = D0;
+        uint32_t mask = mask0;
+        const uint32_t s = window_of_slot<B>(D, mask, g);
         const int cx = D.gx0 + (int)(s % D.nx), cy = D.gy0 + (int)((s / D.nx) % D.ny), cz = D.gz0 + (int)(s / (D.nx * D.ny));
         const uint32_t h0 = grid_hash(cx, cy, cz, mask);
         int best = kDcolReach + 1;
@@ -148,7 +226,7 @@ __global__ void __launch_bounds__(128) k_d_dcol(DenseArgs D, uint32_t mask, uint
                 }
             }
         }
-        dcol[s] = (uint8_t)best;
+        dcol[g] = (uint8_t)best;
     }
 }
 
@@ -394,7 +472,7 @@ __device__ __forceinline__ int interior_slot(const DevParams& P, const DenseArgs
     const uint32_t uy = (uint32_t)cell_coord(xi.y, P.h) - (uint32_t)D.gy0;
     const uint32_t uz = (uint32_t)cell_coord(xi.z, P.h) - (uint32_t)D.gz0;
     if (ux - 1u < D.nx - 2u && uy - 1u < D.ny - 2u && uz - 1u < D.nz - 2u)
-        return (int)((uz * D.ny + uy) * D.nx + ux);
+        return (int)(D.slot0 + (uz * D.ny + uy) * D.nx + ux);
     return -1;
 }
 
@@ -492,8 +570,8 @@ __device__ __forceinline__ void check_drift(const DevParams& P, const DenseArgs&
     const float dx = x.x - b.x, dy = x.y - b.y, dz = x.z - b.z;
     // NaN positions count as moved (the comparison is false for NaN)
     if (!(dx * dx + dy * dy + dz * dz <= D.drift2))
-        settle_drift(D.dcol, D.dirty, D.flag, P.h, P.mask, x.x, x.y, x.z, b.x, b.y, b.z, D.gx0, D.gy0, D.gz0, D.nx, D.ny,
-                     D.nz);
+        settle_drift(D.dcol + D.slot0, D.dirty + D.slot0, D.flag, P.h, P.mask, x.x, x.y, x.z, b.x, b.y, b.z, D.gx0,
+                     D.gy0, D.gz0, D.nx, D.ny, D.nz);
 }
 
 // ---- thread order by current cell ----------------------------------------------------------
@@ -520,19 +598,25 @@ __device__ __forceinline__ void slot_run(uint32_t s, uint32_t lane, uint32_t& he
 
 constexpr uint32_t kNoSlot = 0xffffffffu;
 
-// slot of the current cell (cells outside the window interior: one extra slot)
-__global__ void __launch_bounds__(256) k_d_cslot(DevParams P, DenseArgs D, const float4* __restrict__ X,
+// Global slot of the cell of x (cells outside the window: the extra slot D.total).
+__device__ __forceinline__ uint32_t current_slot(const DevParams& P, const DenseArgs& D, float4 x)
+{
+    const uint32_t ux = (uint32_t)cell_coord(x.x, P.h) - (uint32_t)D.gx0;
+    const uint32_t uy = (uint32_t)cell_coord(x.y, P.h) - (uint32_t)D.gy0;
+    const uint32_t uz = (uint32_t)cell_coord(x.z, P.h) - (uint32_t)D.gz0;
+    return (ux < D.nx && uy < D.ny && uz < D.nz) ? D.slot0 + (uz * D.ny + uy) * D.nx + ux : D.total;
+}
+
+// slot of the current cell
+template <bool B>
+__global__ void __launch_bounds__(256) k_d_cslot(DevParams P0, DenseArgs D0, const float4* __restrict__ X,
                                                  uint32_t* __restrict__ slot_of, uint32_t* __restrict__ cnt)
 {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t s = kNoSlot;
-    if (t < P.n) {
-        const float4 x = __ldg(X + t);
-        const uint32_t ux = (uint32_t)cell_coord(x.x, P.h) - (uint32_t)D.gx0;
-        const uint32_t uy = (uint32_t)cell_coord(x.y, P.h) - (uint32_t)D.gy0;
-        const uint32_t uz = (uint32_t)cell_coord(x.z, P.h) - (uint32_t)D.gz0;
-        const uint32_t slots = D.nx * D.ny * D.nz;
-        s = (ux < D.nx && uy < D.ny && uz < D.nz) ? (uz * D.ny + uy) * D.nx + ux : slots;
+    if (t < P0.n) {
+        with_scene<B>(P0, D0, (int)t,
+                      [&](const DevParams& P, const DenseArgs& D) { s = current_slot(P, D, __ldg(X + t)); });
         slot_of[t] = s;
     }
     const uint32_t lane = threadIdx.x & 31u;
@@ -548,10 +632,7 @@ __device__ __forceinline__ void record_slot(const DevParams& P, const DenseArgs&
 {
     uint32_t s = kNoSlot;
     if (valid) {
-        const uint32_t ux = (uint32_t)cell_coord(x.x, P.h) - (uint32_t)D.gx0;
-        const uint32_t uy = (uint32_t)cell_coord(x.y, P.h) - (uint32_t)D.gy0;
-        const uint32_t uz = (uint32_t)cell_coord(x.z, P.h) - (uint32_t)D.gz0;
-        s = (ux < D.nx && uy < D.ny && uz < D.nz) ? (uz * D.ny + uy) * D.nx + ux : D.nx * D.ny * D.nz;
+        s = current_slot(P, D, x);
         D.rec_slot[t] = s;
     }
     const uint32_t lane = threadIdx.x & 31u;
@@ -650,105 +731,117 @@ __global__ void __launch_bounds__(256) k_d_place(uint32_t n, const uint32_t* __r
     if (s != kNoSlot) order[__ldg(block_offs + s / kScanItems) + b + (lane - head)] = t;
 }
 
-__global__ void __launch_bounds__(kDThreads) k_d_lambda(DevParams P, DenseArgs D, const float4* __restrict__ lx_in,
+template <bool B>
+__global__ void __launch_bounds__(kDThreads) k_d_lambda(DevParams P0, DenseArgs D0, const float4* __restrict__ lx_in,
                                                         float4* __restrict__ lx_out, float* __restrict__ lrho)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (int)P.n) return;
-    const int t = D.order ? (int)__ldg(D.order + i) : i;
-    const float4 xi = __ldg(lx_in + t);
-    float rho, den;
-    float3 g;
-    float4 out;
-    const int s0 = fast_slot(P, D, xi);
-    if (s0 >= 0) {
-        int q = 0;
-        out = lambda_core(P, GSrc{lx_in}, xi,
-                          RunWalkRec{D.runs, lx_in, xi, t, s0, (int)D.nx, (int)(D.nx * D.ny), D.hm, P.n, &q}, rho, g,
-                          den);
-        D.hcnt[t] = q <= kListChunks ? (uint8_t)q : kNoList;
-    } else {
-        count_bucket_walk(D);
-        out = lambda_core(P, GSrc{lx_in}, xi, BucketWalkLabels{P, D.htable, D.inv, lx_in, xi, t}, rho, g, den);
-        D.hcnt[t] = kNoList;
-    }
-    lx_out[t] = out;
-    lrho[t] = rho;
+    if (i >= (int)P0.n) return;
+    const int t = D0.order ? (int)__ldg(D0.order + i) : i;
+    with_scene<B>(P0, D0, t, [&](const DevParams& P, const DenseArgs& D) {
+        const float4 xi = __ldg(lx_in + t);
+        float rho, den;
+        float3 g;
+        float4 out;
+        const int s0 = fast_slot(P, D, xi);
+        if (s0 >= 0) {
+            int q = 0;
+            out = lambda_core(P, GSrc{lx_in}, xi,
+                              RunWalkRec{D.runs, lx_in, xi, t, s0, (int)D.nx, (int)(D.nx * D.ny), D.hm, P.n, &q}, rho, g,
+                              den);
+            D.hcnt[t] = q <= kListChunks ? (uint8_t)q : kNoList;
+        } else {
+            count_bucket_walk(D);
+            out = lambda_core(P, GSrc{lx_in}, xi, BucketWalkLabels{P, D.htable, D.inv, lx_in, xi, t}, rho, g, den);
+            D.hcnt[t] = kNoList;
+        }
+        lx_out[t] = out;
+        lrho[t] = rho;
+    });
 }
 
-__global__ void __launch_bounds__(kDThreads, 10) k_d_deltap(DevParams P, DenseArgs D, const float4* __restrict__ lx_in,
+template <bool B>
+__global__ void __launch_bounds__(kDThreads, 10) k_d_deltap(DevParams P0, DenseArgs D0, const float4* __restrict__ lx_in,
                                                         float4* __restrict__ lx_out)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = i < (int)P.n;
-    const int t = live ? (D.order ? (int)__ldg(D.order + i) : i) : 0;
-    float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (live) {
-        const float4 xi = __ldg(lx_in + t);
-        float3 dp;
-        if (D.use_list && __ldg(D.hcnt + t) != kNoList) {
-            // the lambda pass of this iteration walked this particle's runs
-            const int s0 = interior_slot(P, D, xi);
-            out = deltap_core(P, P.sdf, GSrc{lx_in}, xi,
-                              RunWalkList{D.runs, lx_in, xi, t, s0, (int)D.nx, (int)(D.nx * D.ny), D.hm, P.n}, dp);
-        } else {
-            with_dense_walker(P, D, lx_in, xi, t,
-                              [&](auto&& walk) { out = deltap_core(P, P.sdf, GSrc{lx_in}, xi, walk, dp); });
+    const bool live = i < (int)P0.n;
+    const int t = live ? (D0.order ? (int)__ldg(D0.order + i) : i) : 0;
+    with_scene<B>(P0, D0, t, [&](const DevParams& P, const DenseArgs& D) {
+        float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (live) {
+            const float4 xi = __ldg(lx_in + t);
+            float3 dp;
+            if (D.use_list && __ldg(D.hcnt + t) != kNoList) {
+                // the lambda pass of this iteration walked this particle's runs
+                const int s0 = interior_slot(P, D, xi);
+                out = deltap_core(P, P.sdf, GSrc{lx_in}, xi,
+                                  RunWalkList{D.runs, lx_in, xi, t, s0, (int)D.nx, (int)(D.nx * D.ny), D.hm, P.n}, dp);
+            } else {
+                with_dense_walker(P, D, lx_in, xi, t,
+                                  [&](auto&& walk) { out = deltap_core(P, P.sdf, GSrc{lx_in}, xi, walk, dp); });
+            }
+            lx_out[t] = out;
+            check_drift(P, D, out, t);
         }
-        lx_out[t] = out;
-        check_drift(P, D, out, t);
-    }
-    if (D.rec_cnt) record_slot(P, D, out, t, live);
+        if (D.rec_cnt) record_slot(P, D, out, t, live);
+    });
 }
 
-__global__ void __launch_bounds__(kDThreads, 10) k_d_integrate(DevParams P, DenseArgs D, const float4* __restrict__ lx,
+template <bool B>
+__global__ void __launch_bounds__(kDThreads, 10) k_d_integrate(DevParams P0, DenseArgs D0, const float4* __restrict__ lx,
                                                            const float4* __restrict__ lv, float4* __restrict__ lx0,
                                                            float4* __restrict__ lom,
                                                            const uint32_t* __restrict__ lid, float4* __restrict__ pos,
                                                            float4* __restrict__ vel)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = i < (int)P.n;
-    const int t = live ? (D.order ? (int)__ldg(D.order + i) : i) : 0;
-    float4 xo = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (live) {
-        const float4 x4 = __ldg(lx + t);
-        const float4 v0 = __ldg(lv + t);
-        const float4 p0 = lx0[t];
-        float4 vo, om;
-        with_dense_walker(P, D, lx, x4, t, [&](auto&& walk) {
-            integrate_core(P, P.bmin, P.bmax, P.sdf, GSrc{lx}, GSrc{lv}, x4, v0, p0, walk, xo, vo, om);
-        });
-        if (P.vort_on) lom[t] = om;
-        const uint32_t id = __ldg(lid + t);
-        pos[id] = xo;
-        vel[id] = vo;
-        lx0[t] = xo;
-        check_drift(P, D, xo, t);
-    }
-    if (D.rec_cnt) record_slot(P, D, xo, t, live);
+    const bool live = i < (int)P0.n;
+    const int t = live ? (D0.order ? (int)__ldg(D0.order + i) : i) : 0;
+    with_scene<B>(P0, D0, t, [&](const DevParams& P, const DenseArgs& D) {
+        float4 xo = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (live) {
+            const float4 x4 = __ldg(lx + t);
+            const float4 v0 = __ldg(lv + t);
+            const float4 p0 = lx0[t];
+            float4 vo, om;
+            with_dense_walker(P, D, lx, x4, t, [&](auto&& walk) {
+                integrate_core(P, P.bmin, P.bmax, P.sdf, GSrc{lx}, GSrc{lv}, x4, v0, p0, walk, xo, vo, om);
+            });
+            if (P.vort_on) lom[t] = om;
+            const uint32_t id = __ldg(lid + t);
+            pos[id] = xo;
+            vel[id] = vo;
+            lx0[t] = xo;
+            check_drift(P, D, xo, t);
+        }
+        if (D.rec_cnt) record_slot(P, D, xo, t, live);
+    });
 }
 
-__global__ void __launch_bounds__(kDThreads, 12) k_d_vorticity(DevParams P, DenseArgs D, const float4* __restrict__ lx0,
+template <bool B>
+__global__ void __launch_bounds__(kDThreads, 12) k_d_vorticity(DevParams P0, DenseArgs D0, const float4* __restrict__ lx0,
                                                            const float4* __restrict__ lom,
                                                            const uint32_t* __restrict__ lid, float4* __restrict__ vel)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (int)P.n) return;
-    const int t = D.order ? (int)__ldg(D.order + i) : i;
-    const float4 xi = __ldg(lx0 + t);
-    float3 dv;
-    bool any = false;
-    with_dense_walker(P, D, lx0, xi, t, [&](auto&& walk) {
-        any = vorticity_core(P, GSrc{lx0}, GMag{lom}, xi, __ldg(lom + t), walk, dv);
+    if (i >= (int)P0.n) return;
+    const int t = D0.order ? (int)__ldg(D0.order + i) : i;
+    with_scene<B>(P0, D0, t, [&](const DevParams& P, const DenseArgs& D) {
+        const float4 xi = __ldg(lx0 + t);
+        float3 dv;
+        bool any = false;
+        with_dense_walker(P, D, lx0, xi, t, [&](auto&& walk) {
+            any = vorticity_core(P, GSrc{lx0}, GMag{lom}, xi, __ldg(lom + t), walk, dv);
+        });
+        if (!any) return;
+        const uint32_t id = __ldg(lid + t);
+        float4 v = vel[id];
+        v.x += dv.x;
+        v.y += dv.y;
+        v.z += dv.z;
+        vel[id] = v;
     });
-    if (!any) return;
-    const uint32_t id = __ldg(lid + t);
-    float4 v = vel[id];
-    v.x += dv.x;
-    v.y += dv.y;
-    v.z += dv.z;
-    vel[id] = v;
 }
 
 // ---- launchers ------------------------------------------------------------------------------
@@ -759,24 +852,33 @@ static inline unsigned capped_grid(uint32_t n, uint32_t threads, int sms, uint32
     return want < 1 ? 1 : (want > cap ? cap : want);
 }
 
+// B = true for the scenes of a batch
+#define PBF_DENSE_LAUNCH(KERNEL, GRID, BLOCK, ...)                                                 \
+    do {                                                                                          \
+        if (D.scenes)                                                                             \
+            KERNEL<true><<<(GRID), (BLOCK), 0, st>>>(__VA_ARGS__);                                \
+        else                                                                                      \
+            KERNEL<false><<<(GRID), (BLOCK), 0, st>>>(__VA_ARGS__);                               \
+    } while (0)
+
 void launch_d_keys(const DevParams& P, const DenseArgs& D, const float4* sx, uint32_t* dkey, int sms, cudaStream_t st)
 {
-    k_d_keys<<<capped_grid(P.n, 256, sms, 8), 256, 0, st>>>(P, D, sx, dkey);
+    PBF_DENSE_LAUNCH(k_d_keys, capped_grid(P.n, 256, sms, 8), 256, P, D, sx, dkey);
 }
 
 void launch_d_clean(const DenseArgs& D, uint32_t mask, uint8_t* clean, uint32_t* unclean, int sms, cudaStream_t st)
 {
-    k_d_clean<<<capped_grid(D.nx * D.ny * D.nz, 128, sms, 16), 128, 0, st>>>(D, mask, clean, unclean);
+    PBF_DENSE_LAUNCH(k_d_clean, capped_grid(D.total, 128, sms, 16), 128, D, mask, clean, unclean);
 }
 
 void launch_d_runs(const DenseArgs& D, const int2* cells, int2* runs, int sms, cudaStream_t st)
 {
-    k_d_runs<<<capped_grid(D.nx * D.ny * D.nz, 256, sms, 8), 256, 0, st>>>(D, cells, runs);
+    PBF_DENSE_LAUNCH(k_d_runs, capped_grid(D.total, 256, sms, 8), 256, D, cells, runs);
 }
 
 void launch_d_dcol(const DenseArgs& D, uint32_t mask, uint8_t* dcol, int sms, cudaStream_t st)
 {
-    k_d_dcol<<<capped_grid(D.nx * D.ny * D.nz, 128, sms, 16), 128, 0, st>>>(D, mask, dcol);
+    PBF_DENSE_LAUNCH(k_d_dcol, capped_grid(D.total, 128, sms, 16), 128, D, mask, dcol);
 }
 
 uint32_t order_scan_blocks(uint32_t slots) { return (slots + 1u + kScanItems - 1u) / kScanItems; }
@@ -784,11 +886,11 @@ uint32_t order_scan_blocks(uint32_t slots) { return (slots + 1u + kScanItems - 1
 void launch_d_order(const DevParams& P, const DenseArgs& D, const float4* X, uint32_t* slot_of, uint32_t* cnt,
                     uint32_t* block_sums, uint32_t* order, cudaStream_t st, uint64_t* launches)
 {
-    const uint32_t m = D.nx * D.ny * D.nz + 1u;  // slots + the outside slot
-    const uint32_t nb = order_scan_blocks(m - 1u);
+    const uint32_t m = D.total + 1u;  // slots + the outside slot
+    const uint32_t nb = order_scan_blocks(D.total);
     cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * m, st);
     const unsigned g = (P.n + 255u) / 256u;
-    k_d_cslot<<<g, 256, 0, st>>>(P, D, X, slot_of, cnt);
+    PBF_DENSE_LAUNCH(k_d_cslot, g, 256, P, D, X, slot_of, cnt);
     k_d_scan_blocks<<<nb, 1024, 0, st>>>(cnt, m, block_sums);
     k_d_scan_sums<<<1, 1024, 0, st>>>(block_sums, nb);
     k_d_place<<<g, 256, 0, st>>>(P.n, slot_of, cnt, block_sums, order);
@@ -798,8 +900,8 @@ void launch_d_order(const DevParams& P, const DenseArgs& D, const float4* X, uin
 void launch_d_order_recorded(const DevParams& P, const DenseArgs& D, const uint32_t* slot_of, uint32_t* cnt,
                              uint32_t* block_sums, uint32_t* order, cudaStream_t st, uint64_t* launches)
 {
-    const uint32_t m = D.nx * D.ny * D.nz + 1u;
-    const uint32_t nb = order_scan_blocks(m - 1u);
+    const uint32_t m = D.total + 1u;
+    const uint32_t nb = order_scan_blocks(D.total);
     const unsigned g = (P.n + 255u) / 256u;
     k_d_scan_blocks<<<nb, 1024, 0, st>>>(cnt, m, block_sums);
     k_d_scan_sums<<<1, 1024, 0, st>>>(block_sums, nb);
@@ -810,24 +912,26 @@ void launch_d_order_recorded(const DevParams& P, const DenseArgs& D, const uint3
 void launch_d_lambda(const DevParams& P, const DenseArgs& D, const float4* lx_in, float4* lx_out, float* lrho,
                      cudaStream_t st)
 {
-    k_d_lambda<<<dgrid(P.n), kDThreads, 0, st>>>(P, D, lx_in, lx_out, lrho);
+    PBF_DENSE_LAUNCH(k_d_lambda, dgrid(P.n), kDThreads, P, D, lx_in, lx_out, lrho);
 }
 
 void launch_d_deltap(const DevParams& P, const DenseArgs& D, const float4* lx_in, float4* lx_out, cudaStream_t st)
 {
-    k_d_deltap<<<dgrid(P.n), kDThreads, 0, st>>>(P, D, lx_in, lx_out);
+    PBF_DENSE_LAUNCH(k_d_deltap, dgrid(P.n), kDThreads, P, D, lx_in, lx_out);
 }
 
 void launch_d_integrate(const DevParams& P, const DenseArgs& D, const float4* lx, const float4* lv, float4* lx0,
                         float4* lom, const uint32_t* lid, float4* pos, float4* vel, cudaStream_t st)
 {
-    k_d_integrate<<<dgrid(P.n), kDThreads, 0, st>>>(P, D, lx, lv, lx0, lom, lid, pos, vel);
+    PBF_DENSE_LAUNCH(k_d_integrate, dgrid(P.n), kDThreads, P, D, lx, lv, lx0, lom, lid, pos, vel);
 }
 
 void launch_d_vorticity(const DevParams& P, const DenseArgs& D, const float4* lx0, const float4* lom,
                         const uint32_t* lid, float4* vel, cudaStream_t st)
 {
-    k_d_vorticity<<<dgrid(P.n), kDThreads, 0, st>>>(P, D, lx0, lom, lid, vel);
+    PBF_DENSE_LAUNCH(k_d_vorticity, dgrid(P.n), kDThreads, P, D, lx0, lom, lid, vel);
 }
+
+#undef PBF_DENSE_LAUNCH
 
 }  // namespace pbf

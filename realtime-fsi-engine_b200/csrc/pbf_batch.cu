@@ -78,6 +78,7 @@ pbf_batch::~pbf_batch()
     bfree(mcode); bfree(mka); bfree(mia); bfree(mkb); bfree(mib);
     bfree(sx[0]); bfree(sx[1]); bfree(sv); bfree(sx0); bfree(somega); bfree(rho); bfree(lod);
     bfree(save_pos); bfree(save_vel);
+    dense_free();
     ad_free();
     if (stream) cudaStreamDestroy(stream);
 }
@@ -183,6 +184,35 @@ int pbf_batch::upload_scenes()
     // Morton bits per axis: enough for the widest scene, the scene index
     // above them, within 32 bits (wider scenes wrap, which only costs
     // locality).
+    // dense windows (neighbour mode 8): each scene's walls in cells, as the
+    // kernels compute a cell, with kDenseMargin cells of margin (the
+    // single-scene window), one after another in the global slot space
+    std::vector<int> w(7 * scenes.size());
+    uint64_t total = 0;
+    bool fits = true;
+    for (size_t k = 0; k < scenes.size(); ++k) {
+        SceneDev& d = hs[k];
+        uint64_t cells = 1;
+        for (int a = 0; a < 3; ++a) {
+            const float lo = std::floor(d.bmin[a] / h), hi = std::floor(d.bmax[a] / h);
+            const bool ok = lo >= -1e7f && hi <= 1e7f && hi >= lo && hi - lo < 1e6f;
+            fits = fits && ok;
+            d.win_g0[a] = ok ? (int)lo - kDenseMargin : 0;
+            d.win_n[a] = ok ? (uint32_t)((int)hi - (int)lo + 1 + 2 * kDenseMargin) : 1u;
+            cells *= d.win_n[a];
+        }
+        d.slot0 = (uint32_t)std::min<uint64_t>(total, 0xFFFFFFFFull);
+        total = std::min<uint64_t>(total + cells, 1ull << 40);
+        for (int a = 0; a < 3; ++a) {
+            w[7 * k + a] = d.win_g0[a];
+            w[7 * k + 3 + a] = (int)d.win_n[a];
+        }
+        w[7 * k + 6] = (int)d.slot0;
+    }
+    if (!fits) total = 1ull << 40;  // no dense windows (dense_fits() is false)
+    if (w != win || total != dense_total) dense_ready = false;
+    win = w;
+    dense_total = total;
     const uint32_t sbits = ceil_log2(scenes.size());
     mbits = std::min<uint32_t>(std::max<uint32_t>(ceil_log2(max_span), 1u), 10u);
     while (sbits + 3 * mbits > 32) --mbits;
@@ -226,8 +256,168 @@ int pbf_batch::substep_body(const float4* src_pos, const float4* src_vel, float4
     return PBF_OK;
 }
 
+int pbf_batch::effective_mode() const
+{
+    if (neighbour_mode == 4 || neighbour_mode == 8) return neighbour_mode;
+    if (tuned_mode) return tuned_mode;
+    return dense_fits() && n >= (1u << 19) ? 8 : 4;
+}
+
+void pbf_batch::dense_free()
+{
+    bfree(lx[0]); bfree(lx[1]); bfree(lxb); bfree(lv); bfree(lx0); bfree(lom); bfree(lrho);
+    bfree(lid); bfree(lkey); bfree(inv); bfree(dtable); bfree(druns); bfree(dclean); bfree(ddcol);
+    bfree(ddirty); bfree(dhcnt); bfree(dslot_scene); bfree(dflag); bfree(dslot); bfree(dord); bfree(dcnt);
+    bfree(dbsum); bfree(dhm);
+    dense_ready = false;
+}
+
+// Buffers of mode 8 and the per-slot tables that depend only on the windows
+// and hash masks (conditions (a), (b) and the colliding-cell distance of
+// k_dense.cu); called outside graph capture whenever the windows changed.
+int pbf_batch::dense_setup()
+{
+    if (!dense_fits())
+        return set_error(PBF_ERR_INVALID, "dense windows need %llu slots (at most 2^26) and APBF off",
+                         (unsigned long long)dense_total);
+    if (capturing) return set_error(PBF_ERR_STATE, "dense windows changed during graph capture");
+    int rc;
+    const size_t c = std::max<uint32_t>(n, 1u), cp = c + kLabelPad, T = (size_t)dense_total;
+    if (!lx[0]) {
+        if ((rc = balloc(lx[0], cp)) || (rc = balloc(lx[1], cp)) || (rc = balloc(lxb, c)) || (rc = balloc(lv, cp)) ||
+            (rc = balloc(lx0, cp)) || (rc = balloc(lom, cp)) || (rc = balloc(lrho, c)) || (rc = balloc(lid, c)) ||
+            (rc = balloc(lkey, c)) || (rc = balloc(inv, c)) || (rc = balloc(dslot, c)) || (rc = balloc(dord, c)) ||
+            (rc = balloc(dhm, c * kDenseListWords)) || (rc = balloc(dhcnt, c)) || (rc = balloc(dflag, 4))) {
+            dense_free();
+            return rc;
+        }
+    }
+    if ((rc = balloc(dtable, T)) || (rc = balloc(druns, T)) || (rc = balloc(dclean, T)) || (rc = balloc(ddcol, T)) ||
+        (rc = balloc(ddirty, T)) || (rc = balloc(dslot_scene, T)) || (rc = balloc(dcnt, T + 1)) ||
+        (rc = balloc(dbsum, order_scan_blocks((uint32_t)T)))) {
+        dense_free();
+        return rc;
+    }
+    std::vector<uint16_t> ss(T);
+    for (size_t k = 0; k < scenes.size(); ++k) {
+        const size_t b0 = (size_t)(uint32_t)win[7 * k + 6];
+        const size_t cells = (size_t)win[7 * k + 3] * (size_t)win[7 * k + 4] * (size_t)win[7 * k + 5];
+        std::fill(ss.begin() + b0, ss.begin() + b0 + cells, (uint16_t)k);
+    }
+    BCK(cudaMemcpyAsync(dslot_scene, ss.data(), sizeof(uint16_t) * T, cudaMemcpyHostToDevice, stream));
+    BCK(cudaMemsetAsync(dflag, 0, sizeof(uint32_t) * 4, stream));
+    const DenseArgs D = dense_args();
+    launch_d_clean(D, 0u, dclean, dflag + 2, num_sms, stream);
+    launch_d_dcol(D, 0u, ddcol, num_sms, stream);
+    launches += 2;
+    BCK(cudaStreamSynchronize(stream));
+    BCK(cudaGetLastError());
+    dense_ready = true;
+    return PBF_OK;
+}
+
+DenseArgs pbf_batch::dense_args() const
+{
+    DenseArgs D;
+    std::memset(&D, 0, sizeof(D));
+    D.table = dtable;
+    D.runs = druns;
+    D.hm = dhm;
+    D.hcnt = dhcnt;
+    D.clean = dclean;
+    D.dcol = ddcol;
+    D.dirty = ddirty;
+    D.htable = table;
+    D.inv = inv;
+    D.xb = lxb;
+    D.flag = dflag;
+    const float b = 0.9f * derived.h;
+    D.drift2 = b * b;
+    D.total = (uint32_t)dense_total;
+    D.scenes = scenes_dev;
+    D.scene_of = scene_of;
+    D.slot_scene = dslot_scene;
+    return D;
+}
+
+// The step in mode 8: per substep the hashed sort and table (the walk of
+// particles that fail the window conditions), the relabelling by global window
+// slot, then the passes of k_dense.cu over all scenes at once.  Passes after
+// the first iteration take their threads in current-cell order from the
+// slots the previous pass recorded; delta-p replays its lambda's hit masks.
+int pbf_batch::dense_step_body()
+{
+    const DevParams P = dev_params();
+    const int sms = num_sms;
+    const uint32_t T = (uint32_t)dense_total;
+    const uint32_t slot_bits = std::max<uint32_t>(ceil_log2(T), 1u);
+    const uint32_t iters = cfg.solver_iterations;
+    const bool vort = cfg.enable_vorticity;
+    DenseArgs D = dense_args();
+    auto record = [&]() -> int {
+        BCK(cudaMemsetAsync(dcnt, 0, sizeof(uint32_t) * ((size_t)T + 1), stream));
+        D.rec_slot = dslot;
+        D.rec_cnt = dcnt;
+        return PBF_OK;
+    };
+    auto order_recorded = [&]() {
+        launch_d_order_recorded(P, D, dslot, dcnt, dbsum, dord, stream, &launches);
+        D.order = dord;
+    };
+    for (uint32_t sub = 0; sub < cfg.substep_iterations; ++sub) {
+        const bool last = sub + 1 == cfg.substep_iterations;
+        launch_b_predict(P, scenes_dev, scene_of, pos, vel, keys, sms, stream);
+        launch_radix_sort(n, key_bits, keys, ka, ia, kb, ib, hist, totals, &skeys, &ids, stream, &launches);
+        BCK(cudaMemsetAsync(table, 0xFF, sizeof(int2) * (size_t)table_size, stream));
+        launch_build_table(n, skeys, table, sms, stream);
+        launch_b_reorder(P, scenes_dev, scene_of, ids, pos, vel, sx[0], sv, sx0, lod, nullptr, mbits, sms, stream);
+        D = dense_args();
+        launch_d_keys(P, D, sx[0], mcode, sms, stream);
+        launches += 4;
+        uint32_t *msorted = nullptr, *lorder = nullptr;
+        launch_radix_sort(n, slot_bits, mcode, mka, mia, mkb, mib, hist, totals, &msorted, &lorder, stream,
+                          &launches);
+        launch_l_permute(n, lorder, ids, skeys, sx[0], sv, sx0, lx[0], lxb, lv, lx0, lid, lkey, inv, sms, stream);
+        BCK(cudaMemsetAsync(dtable, 0xFF, sizeof(int2) * (size_t)T, stream));
+        launch_build_table(n, msorted, dtable, sms, stream);
+        launch_d_runs(D, dtable, druns, sms, stream);
+        BCK(cudaMemsetAsync(ddirty, 0, (size_t)T, stream));
+        BCK(cudaMemsetAsync(dflag, 0, sizeof(uint32_t), stream));
+        launches += 3;
+        for (uint32_t it = 1; it <= iters; ++it) {
+            D.rec_slot = nullptr;
+            D.rec_cnt = nullptr;
+            D.use_list = 0;
+            if (it >= 2) order_recorded();
+            launch_d_lambda(P, D, lx[0], lx[1], lrho, stream);
+            D.use_list = 1;
+            if (const int rc = record()) return rc;
+            launch_d_deltap(P, D, lx[1], lx[0], stream);
+            launches += 2;
+        }
+        D.rec_slot = nullptr;
+        D.rec_cnt = nullptr;
+        D.use_list = 0;
+        order_recorded();
+        if (last && vort) {
+            if (const int rc = record()) return rc;
+        }
+        launch_d_integrate(P, D, lx[0], lv, lx0, lom, lid, pos, vel, stream);
+        ++launches;
+    }
+    if (vort) {
+        D.rec_slot = nullptr;
+        D.rec_cnt = nullptr;
+        order_recorded();
+        launch_d_vorticity(P, D, lx0, lom, lid, vel, stream);
+        ++launches;
+    }
+    return PBF_OK;
+}
+
 int pbf_batch::step_body()
 {
+    if (effective_mode() == 8) return dense_step_body();
     const DevParams P = dev_params();
     BatchLaunch L = launch;
     L.sms = num_sms;
@@ -245,6 +435,10 @@ int pbf_batch::step_body()
 int pbf_batch::step()
 {
     if (n == 0) return PBF_OK;
+    if (effective_mode() == 8 && !dense_ready) {
+        invalidate_graph();
+        if (const int rc = dense_setup()) return rc;
+    }
     if (use_graph) {
         if (!graph_exec) {
             const uint64_t before = launches;
@@ -540,6 +734,15 @@ extern "C" int pbf_batch_set_option(pbf_batch* b, int option, int value)
     case PBF_BOPT_USE_GRAPH:
         b->use_graph = value != 0;
         break;
+    case PBF_BOPT_NEIGHBOUR_MODE:
+        if (value != -1 && value != 4 && value != 8)
+            return set_error(PBF_ERR_INVALID, "neighbour mode %d not in {-1, 4, 8}", value);
+        if (value == 8 && !b->dense_fits())
+            return set_error(PBF_ERR_INVALID, "dense windows need %llu slots (at most 2^26) and APBF off",
+                             (unsigned long long)b->dense_total);
+        b->neighbour_mode = value;
+        b->tuned_mode = 0;
+        break;
     default:
         return set_error(PBF_ERR_INVALID, "unknown batch option %d", option);
     }
@@ -555,15 +758,17 @@ extern "C" int pbf_batch_get_option(const pbf_batch* b, int option, int* value)
     case PBF_BOPT_ORDER: *value = b->morton; break;
     case PBF_BOPT_BLOCKS_PER_SM: *value = b->launch.blocks_per_sm; break;
     case PBF_BOPT_USE_GRAPH: *value = b->use_graph ? 1 : 0; break;
+    case PBF_BOPT_NEIGHBOUR_MODE: *value = b->neighbour_mode; break;
     default: return set_error(PBF_ERR_INVALID, "unknown batch option %d", option);
     }
     return PBF_OK;
 }
 
-// Autotuner: every (block, order, persistence) candidate is timed with CUDA
-// events over `trial_steps` graph replays after one warm-up replay (which
-// also captures the graph); the particle state is saved before and restored
-// after, so tuning leaves the simulation where it was.
+// Autotuner: every candidate (neighbour mode 8 when the windows fit; block x
+// order x persistence in mode 4) is timed with CUDA events over `trial_steps`
+// graph replays after one warm-up replay (which also captures the graph); the
+// particle state is saved before and restored after, so tuning leaves the
+// simulation where it was.
 extern "C" int pbf_batch_autotune(pbf_batch* b, uint32_t trial_steps, pbf_batch_tuning* best,
                                   pbf_batch_tuning* results, uint32_t max_results, uint32_t* num_results)
 {
@@ -582,10 +787,37 @@ extern "C" int pbf_batch_autotune(pbf_batch* b, uint32_t trial_steps, pbf_batch_
     cudaEvent_t e0, e1;
     BCK(cudaEventCreate(&e0));
     BCK(cudaEventCreate(&e1));
-    pbf_batch_tuning pick{b->launch.block, b->morton, b->launch.blocks_per_sm, 1e30f};
+    pbf_batch_tuning pick{b->launch.block, b->morton, b->launch.blocks_per_sm, 1e30f, 4};
     uint32_t count = 0;
     const int blocks[3] = {64, 128, 256};
-    for (int order = 0; order <= 1 && !rc; ++order) {
+    const int mode_was = b->neighbour_mode;
+    auto time_steps = [&](float* ms) -> int {
+        b->invalidate_graph();
+        int r = b->step();
+        if (r) return r;
+        cudaEventRecord(e0, b->stream);
+        for (uint32_t i = 0; i < trial_steps && !r; ++i) r = b->step();
+        cudaEventRecord(e1, b->stream);
+        if (r) return r;
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) return set_error(PBF_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
+        cudaEventElapsedTime(ms, e0, e1);
+        *ms /= (float)trial_steps;
+        return PBF_OK;
+    };
+    if (mode_was != 4 && b->dense_fits()) {
+        b->neighbour_mode = 8;
+        float ms = 0.0f;
+        rc = time_steps(&ms);
+        if (!rc) {
+            const pbf_batch_tuning r{b->launch.block, b->morton, b->launch.blocks_per_sm, ms, 8};
+            if (results && count < max_results) results[count] = r;
+            ++count;
+            pick = r;
+        }
+    }
+    b->neighbour_mode = 4;
+    for (int order = 0; order <= 1 && !rc && mode_was != 8; ++order) {
         for (int bi = 0; bi < 3 && !rc; ++bi) {
             const int occ = batch_max_blocks_per_sm(blocks[bi]);
             const int bps_list[2] = {0, occ};
@@ -593,20 +825,9 @@ extern "C" int pbf_batch_autotune(pbf_batch* b, uint32_t trial_steps, pbf_batch_
                 b->launch.block = blocks[bi];
                 b->morton = order;
                 b->launch.blocks_per_sm = bps_list[pi];
-                b->invalidate_graph();
-                if ((rc = b->step())) break;
-                cudaEventRecord(e0, b->stream);
-                for (uint32_t i = 0; i < trial_steps && !rc; ++i) rc = b->step();
-                cudaEventRecord(e1, b->stream);
-                if (rc) break;
-                cudaError_t e = cudaEventSynchronize(e1);
-                if (e != cudaSuccess) {
-                    rc = set_error(PBF_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
-                    break;
-                }
                 float ms = 0.0f;
-                cudaEventElapsedTime(&ms, e0, e1);
-                const pbf_batch_tuning r{blocks[bi], order, bps_list[pi], ms / (float)trial_steps};
+                if ((rc = time_steps(&ms))) break;
+                const pbf_batch_tuning r{blocks[bi], order, bps_list[pi], ms, 4};
                 if (results && count < max_results) results[count] = r;
                 ++count;
                 if (r.ms_per_step < pick.ms_per_step) pick = r;
@@ -618,6 +839,8 @@ extern "C" int pbf_batch_autotune(pbf_batch* b, uint32_t trial_steps, pbf_batch_
     b->launch.block = pick.block;
     b->morton = pick.order;
     b->launch.blocks_per_sm = pick.blocks_per_sm;
+    b->neighbour_mode = mode_was;
+    b->tuned_mode = mode_was == -1 ? pick.neighbour_mode : 0;
     b->use_graph = graph_was;
     b->invalidate_graph();
     BCK(cudaMemcpyAsync(b->pos, b->save_pos, sizeof(float4) * c, cudaMemcpyDeviceToDevice, b->stream));

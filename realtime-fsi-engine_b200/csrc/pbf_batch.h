@@ -19,7 +19,34 @@ struct SceneDev {
     int cell_lo[3];      // lowest cell of the walls: origin of the Morton code
     int pad_;
     SdfDev sdf;
+    // dense window (neighbour mode 8): cell of window slot (0, 0, 0), extent,
+    // first global slot
+    int win_g0[3];
+    uint32_t win_n[3];
+    uint32_t slot0;
 };
+
+#ifdef __CUDACC__
+// The SDF of scene S as the passes sample it.
+__device__ __forceinline__ SdfDev load_sdf(const SceneDev* S)
+{
+    SdfDev d;
+    d.enabled = __ldg(&S->sdf.enabled);
+    d.dist = S->sdf.dist;
+    d.slab_min = S->sdf.slab_min;
+    d.dx = __ldg(&S->sdf.dx);
+    d.dy = __ldg(&S->sdf.dy);
+    d.dz = __ldg(&S->sdf.dz);
+    d.ox = __ldg(&S->sdf.ox);
+    d.oy = __ldg(&S->sdf.oy);
+    d.oz = __ldg(&S->sdf.oz);
+    d.cell = __ldg(&S->sdf.cell);
+    d.inv_cell = __ldg(&S->sdf.inv_cell);
+    d.padding = __ldg(&S->sdf.padding);
+    d.containment = __ldg(&S->sdf.containment);
+    return d;
+}
+#endif
 
 struct BatchLaunch {
     int block = 128;         // threads per block of the neighbour passes
@@ -121,6 +148,23 @@ struct pbf_batch {
     pbf::BatchLaunch launch{};
     int morton = 1;
     bool use_graph = true;
+    int neighbour_mode = -1;  // -1 automatic, 4 hashed buckets, 8 dense windows
+    int tuned_mode = 0;       // the autotuner's pick under -1 (0: none yet)
+
+    // neighbour mode 8 (k_dense.cu): a dense cell window per scene, scene k's
+    // window at global slots [SceneDev::slot0, + its cells); labels sorted by
+    // (global slot of the predict-time cell, hash-sorted index), scene-contiguous
+    std::vector<int> win;         // per scene: g0[3], n[3], slot0 (7 ints), as uploaded
+    uint64_t dense_total = 0;     // slots of all windows
+    bool dense_ready = false;     // the clean/dcol tables below match `win` and the hash masks
+    float4 *lx[2] = {nullptr, nullptr}, *lxb = nullptr, *lv = nullptr, *lx0 = nullptr, *lom = nullptr;
+    float* lrho = nullptr;
+    uint32_t *lid = nullptr, *lkey = nullptr, *inv = nullptr;
+    int2 *dtable = nullptr, *druns = nullptr;
+    uint8_t *dclean = nullptr, *ddcol = nullptr, *ddirty = nullptr, *dhcnt = nullptr;
+    uint16_t* dslot_scene = nullptr;
+    uint32_t *dflag = nullptr, *dslot = nullptr, *dord = nullptr, *dcnt = nullptr, *dbsum = nullptr;
+    uint32_t* dhm = nullptr;
 
     uint64_t launches = 0;
     bool capturing = false;
@@ -146,6 +190,12 @@ struct pbf_batch {
 
     ~pbf_batch();
     pbf::DevParams dev_params() const;
+    bool dense_fits() const { return dense_total > 0 && dense_total <= (1ull << 26) && !derived.enable_apbf; }
+    int effective_mode() const;
+    int dense_setup();
+    void dense_free();
+    pbf::DenseArgs dense_args() const;
+    int dense_step_body();
     int upload_scenes();
     void invalidate_graph();
     int step_body();

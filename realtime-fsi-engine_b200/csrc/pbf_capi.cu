@@ -413,12 +413,11 @@ int pbf_handle::ensure_label_capacity()
 
 // ---- dense cell window (mode 8) -----------------------------------------------------------
 // The walls' box in cells (floor(x / h) in FP32, as the kernels compute a
-// cell) with kWindowMargin cells of margin on each side.  Any window is
+// cell) with kDenseMargin cells of margin on each side.  Any window is
 // correct (cells outside wrap into it and their queries walk the hashed
 // buckets); the margin also holds the predict-time cells of particles that
 // move towards a wall (x* = x + v dt lies beyond it until the walls clamp
 // it), whose later correction would otherwise count as an unchecked drift.
-constexpr int kWindowMargin = 6;
 
 bool pbf_handle::dense_window(int g0[3], uint32_t nd[3]) const
 {
@@ -428,8 +427,8 @@ bool pbf_handle::dense_window(int g0[3], uint32_t nd[3]) const
     for (int a = 0; a < 3; ++a) {
         const float lo = std::floor(derived.bounds_min[a] / h), hi = std::floor(derived.bounds_max[a] / h);
         if (!(lo >= -1e8f && hi <= 1e8f && hi >= lo)) return false;
-        g0[a] = (int)lo - kWindowMargin;
-        nd[a] = (uint32_t)((int)hi - (int)lo + 1 + 2 * kWindowMargin);
+        g0[a] = (int)lo - kDenseMargin;
+        nd[a] = (uint32_t)((int)hi - (int)lo + 1 + 2 * kDenseMargin);
         slots *= nd[a];
     }
     return slots <= (1ull << 26);
@@ -461,6 +460,11 @@ DenseArgs pbf_handle::dense_args() const
     D.nz = dwin_n[2];
     const float b = 0.9f * derived.h;
     D.drift2 = b * b;
+    D.slot0 = 0;
+    D.total = dwin_n[0] * dwin_n[1] * dwin_n[2];
+    D.scenes = nullptr;
+    D.scene_of = nullptr;
+    D.slot_scene = nullptr;
     return D;
 }
 

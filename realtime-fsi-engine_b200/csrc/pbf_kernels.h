@@ -132,6 +132,15 @@ constexpr int kDenseListWords = 16;
 // Label-space position/velocity arrays hold this many entries past the last
 // label, so a run's last chunk of candidates may load past the run's end.
 constexpr int kLabelPad = 32;
+// Cells of margin around the walls' box in a dense window: they also hold the
+// predict-time cells of particles that move towards a wall (x* = x + v dt lies
+// beyond it until the walls clamp it).
+constexpr int kDenseMargin = 6;
+struct SceneDev;  // pbf_batch.h
+// A dense window per scene: one scene (scenes == null), or the scenes of a
+// batch, scene k's window occupying global slots [slot0_k, slot0_k + its
+// cells).  The window fields below describe one window; the passes of a batch
+// replace them, the hash mask, walls and SDF with the scene of each label.
 struct DenseArgs {
     const int2* table;     // per window slot: label range of its particles, (-1, -1) when empty
     const int2* runs;      // per window slot: label range of slots s-1 .. s+1 of its row
@@ -151,6 +160,11 @@ struct DenseArgs {
     int gx0, gy0, gz0;     // cell coordinates of window slot (0, 0, 0)
     uint32_t nx, ny, nz;   // window extent in cells
     float drift2;          // squared drift bound (0.9 h)^2
+    uint32_t slot0;        // global slot of window slot (0, 0, 0)
+    uint32_t total;        // slots of all windows (the thread order's extra slot is `total`)
+    const SceneDev* scenes;      // batch: per-scene constants (null: one scene)
+    const uint16_t* scene_of;    // batch: scene of each label / hash-sorted index (scene-contiguous)
+    const uint16_t* slot_scene;  // batch: scene of each global slot
 };
 void launch_d_keys(const DevParams& P, const DenseArgs& D, const float4* sx, uint32_t* dkey, int sms, cudaStream_t st);
 void launch_d_clean(const DenseArgs& D, uint32_t mask, uint8_t* clean, uint32_t* unclean, int sms, cudaStream_t st);

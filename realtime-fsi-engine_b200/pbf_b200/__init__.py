@@ -14,7 +14,8 @@ import numpy as np
 from ._capi import (BUF_KEYS, BUF_LOD, BUF_OMEGA, BUF_POS, BUF_RHO, BUF_SORTED_IDS, BUF_SORTED_KEYS, BUF_TABLE,
                     BUF_VEL, BUF_VPRED, BUF_XSTAR, NUM_PASS_SLOTS, PASS_NAMES, STAGE_DELTAP, STAGE_INTEGRATE,
                     STAGE_LAMBDA, STAGE_PREDICT, STAGE_REORDER, STAGE_SORT, STAGE_TABLE, STAGE_VORTICITY,
-                    BATCH_ALL, BOPT_BLOCK, BOPT_BLOCKS_PER_SM, BOPT_ORDER, BOPT_USE_GRAPH, BatchTuning,
+                    BATCH_ALL, BOPT_BLOCK, BOPT_BLOCKS_PER_SM, BOPT_NEIGHBOUR_MODE, BOPT_ORDER, BOPT_USE_GRAPH,
+                    BatchTuning,
                     ContactCandidate, DerivedParams, FluidConfig, Particle, PBFError, SceneDesc, check, fvec, lib)
 
 # numpy view of Particle (48 bytes: pos, pad0, predPos, pad1, vel, pad2)
@@ -479,7 +480,8 @@ class Batch:
         return v.value
 
     def autotune(self, trial_steps=3):
-        """Pick block size, cell order and persistence by timing; returns
+        """Pick the neighbour mode (dense windows or hashed buckets) and, for
+        the buckets, block size, cell order and persistence by timing; returns
         (best, [all candidates]) as dicts.  The particle state is restored."""
         best = BatchTuning()
         res = (BatchTuning * 32)()
@@ -488,7 +490,8 @@ class Batch:
                                        C.byref(cnt)))
 
         def d(t):
-            return dict(block=t.block, order=t.order, blocks_per_sm=t.blocks_per_sm, ms_per_step=t.ms_per_step)
+            return dict(block=t.block, order=t.order, blocks_per_sm=t.blocks_per_sm, ms_per_step=t.ms_per_step,
+                        neighbour_mode=t.neighbour_mode)
 
         return d(best), [d(res[i]) for i in range(cnt.value)]
 
@@ -537,7 +540,7 @@ __all__ = [
     "PBFluids", "SDFBoundary", "GridSDF", "FluidConfig", "DerivedParams", "Particle", "ContactCandidate",
     "PARTICLE_DTYPE", "CONTACT_DTYPE", "default_config", "derive_params", "make_particles", "sort_keys",
     "build_table", "PBFError", "lib", "Batch", "SceneDesc", "BATCH_ALL", "BOPT_BLOCK", "BOPT_ORDER",
-    "BOPT_BLOCKS_PER_SM", "BOPT_USE_GRAPH",
+    "BOPT_BLOCKS_PER_SM", "BOPT_USE_GRAPH", "BOPT_NEIGHBOUR_MODE",
     "STAGE_PREDICT", "STAGE_SORT", "STAGE_TABLE", "STAGE_REORDER", "STAGE_LAMBDA", "STAGE_DELTAP",
     "STAGE_INTEGRATE", "STAGE_VORTICITY", "BUF_KEYS", "BUF_SORTED_KEYS", "BUF_SORTED_IDS", "BUF_TABLE",
     "BUF_XSTAR", "BUF_VPRED", "BUF_RHO", "BUF_OMEGA", "BUF_POS", "BUF_VEL", "BUF_LOD",

@@ -86,7 +86,7 @@ class BatchTuning(C.Structure):
     """pbf_batch_tuning: one autotuner candidate and its time per step."""
 
     _fields_ = [("block", C.c_int32), ("order", C.c_int32), ("blocks_per_sm", C.c_int32),
-                ("ms_per_step", C.c_float)]
+                ("ms_per_step", C.c_float), ("neighbour_mode", C.c_int32)]
 
 
 class DeformParams(C.Structure):
@@ -98,11 +98,11 @@ class DeformParams(C.Structure):
 
 
 BATCH_ALL = 0xFFFFFFFF
-BOPT_BLOCK, BOPT_ORDER, BOPT_BLOCKS_PER_SM, BOPT_USE_GRAPH = 1, 2, 3, 4
+BOPT_BLOCK, BOPT_ORDER, BOPT_BLOCKS_PER_SM, BOPT_USE_GRAPH, BOPT_NEIGHBOUR_MODE = 1, 2, 3, 4, 5
 
 assert C.sizeof(Particle) == 48 and C.sizeof(ContactCandidate) == 32
 assert C.sizeof(DerivedParams) == 144
-assert C.sizeof(SceneDesc) == 32 and C.sizeof(BatchTuning) == 16
+assert C.sizeof(SceneDesc) == 32 and C.sizeof(BatchTuning) == 20
 
 vp = C.c_void_p
 i32 = C.c_int32

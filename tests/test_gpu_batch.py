@@ -91,7 +91,8 @@ def test_autotune_restores_state_and_reports_candidates(have_gpu):
     best, cands = b.autotune(2)
     after = b.read_particles()
     assert np.array_equal(before["pos"], after["pos"]) and np.array_equal(before["vel"], after["vel"])
-    assert len(cands) == 12
+    # 12 launch shapes of the hashed-bucket walk and the dense windows
+    assert len(cands) == 13 and sorted(c["neighbour_mode"] for c in cands) == [4] * 12 + [8]
     assert best["ms_per_step"] == min(c["ms_per_step"] for c in cands)
     assert b.get_option(P.BOPT_BLOCK) == best["block"] and b.get_option(P.BOPT_ORDER) == best["order"]
     # stepping on with the tuned options continues the same trajectory
@@ -103,6 +104,53 @@ def test_autotune_restores_state_and_reports_candidates(have_gpu):
     a = b.read_particles()
     r = ref.read_particles()
     assert np.array_equal(a["pos"], r["pos"])
+
+
+@pytest.mark.parametrize("graph", [1, 0])
+def test_dense_windows_are_bit_identical_to_buckets(have_gpu, graph):
+    """Neighbour mode 8 (a dense cell window per scene, the passes over all
+    scenes at once) gives the bits of the hashed-bucket walk, over steps in
+    which the particles fall, splash and collide with each scene's sphere."""
+    cfg, sc = small_c3(sizes=[1500, 3200, 700, 5000, 64, 9000])
+    base = run_batch(cfg, sc, 6, [(P.BOPT_NEIGHBOUR_MODE, 4)])
+    got = run_batch(cfg, sc, 6, [(P.BOPT_NEIGHBOUR_MODE, 8), (P.BOPT_USE_GRAPH, graph)])
+    assert np.array_equal(got["pos"], base["pos"]) and np.array_equal(got["vel"], base["vel"])
+
+
+def test_dense_windows_with_hash_collisions(have_gpu):
+    """Small per-scene hash tables (different per scene) make many cells share
+    buckets: those cells walk their scene's hashed buckets inside the dense
+    passes, still bit-identical to the hashed-bucket walk."""
+    cfg, sc = small_c3()
+    for k, s in enumerate(sc):
+        s["hash_size"] = [256, 4096, 1024, 2048, 64][k]
+    base = run_batch(cfg, sc, 4, [(P.BOPT_NEIGHBOUR_MODE, 4)])
+    got = run_batch(cfg, sc, 4, [(P.BOPT_NEIGHBOUR_MODE, 8)])
+    assert np.array_equal(got["pos"], base["pos"]) and np.array_equal(got["vel"], base["vel"])
+
+
+def test_dense_windows_match_one_handle_per_scene(have_gpu):
+    cfg, sc = small_c3()
+    got = run_batch(cfg, sc, 3, [(P.BOPT_NEIGHBOUR_MODE, 8)])
+    off = 0
+    for (f, _), s in zip(PB.make_sequential(cfg, sc), sc):
+        f.set_option(1, 8)
+        for _ in range(3):
+            f.step()
+        ref = f.readbackParticles()
+        mine = got[off:off + s["n"]]
+        off += s["n"]
+        assert np.abs(mine["pos"] - ref["pos"]).max() <= 1e-6 * cfg.h
+
+
+def test_neighbour_mode_option(have_gpu):
+    cfg, sc = small_c3()
+    b = PB.make_batch(cfg, sc)
+    assert b.get_option(P.BOPT_NEIGHBOUR_MODE) == -1
+    b.set_option(P.BOPT_NEIGHBOUR_MODE, 8)
+    assert b.get_option(P.BOPT_NEIGHBOUR_MODE) == 8
+    with pytest.raises(P.PBFError):
+        b.set_option(P.BOPT_NEIGHBOUR_MODE, 6)
 
 
 def test_per_scene_io_and_errors(have_gpu):
