@@ -265,6 +265,19 @@ __device__ __forceinline__ void masked_range(const float4* __restrict__ X, float
     }
 }
 
+// (a.x - b.x, a.y - b.y) in one packed instruction, each lane rounded as a
+// scalar FP32 subtraction is.
+__device__ __forceinline__ float2 sub_f32x2(float2 a, float2 b)
+{
+    uint64_t ua, ub, r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(ua) : "f"(a.x), "f"(a.y));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(ub) : "f"(b.x), "f"(b.y));
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(ua), "l"(ub));
+    float2 o;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(o.x), "=f"(o.y) : "l"(r));
+    return o;
+}
+
 // masked_range for candidates that are labels (a run): the query's own label
 // is cleared from each chunk's mask once instead of being compared with every
 // candidate.
@@ -274,6 +287,7 @@ __device__ __forceinline__ void label_range(const float4* __restrict__ X, float4
 {
     static_assert(C >= 1 && C <= 32, "hit mask is 32 bits");
     constexpr int G = 32 / C;  // chunks tested before one drain of up to 32 candidates
+    const float2 xy = make_float2(xi.x, xi.y);
 #pragma unroll 1
     for (int k0 = lo; k0 < hi; k0 += G * C) {
         uint32_t m = 0;
@@ -285,7 +299,8 @@ __device__ __forceinline__ void label_range(const float4* __restrict__ X, float4
 #pragma unroll
             for (int c = 0; c < C; ++c) {
                 const float4 xj = __ldg(X + kb + c);
-                const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+                const float2 rxy = sub_f32x2(xy, make_float2(xj.x, xj.y));
+                const float rx = rxy.x, ry = rxy.y, rz = xi.z - xj.z;
                 if (hit(rx * rx + ry * ry + rz * rz)) mg |= 1u << c;
             }
             const uint32_t ds = (uint32_t)(self - kb);
