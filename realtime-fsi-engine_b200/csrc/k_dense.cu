@@ -265,19 +265,6 @@ __device__ __forceinline__ void masked_range(const float4* __restrict__ X, float
     }
 }
 
-// (a.x - b.x, a.y - b.y) in one packed instruction, each lane rounded as a
-// scalar FP32 subtraction is.
-__device__ __forceinline__ float2 sub_f32x2(float2 a, float2 b)
-{
-    uint64_t ua, ub, r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(ua) : "f"(a.x), "f"(a.y));
-    asm("mov.b64 %0, {%1, %2};" : "=l"(ub) : "f"(b.x), "f"(b.y));
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(ua), "l"(ub));
-    float2 o;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(o.x), "=f"(o.y) : "l"(r));
-    return o;
-}
-
 // masked_range for candidates that are labels (a run): the query's own label
 // is cleared from each chunk's mask once instead of being compared with every
 // candidate.

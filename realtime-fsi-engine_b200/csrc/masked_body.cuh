@@ -106,22 +106,26 @@ template <class XS, class Walk>
 __device__ __forceinline__ float4 lambda_core(const DevParams& P, XS X, float4 xi, Walk&& walk, float& rho_out,
                                               float3& g_out, float& den_out)
 {
-    float rho = P.w0_self, sg = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+    float rho = P.w0_self, sg = 0.f, gz = 0.f;
+    float2 gxy = make_float2(0.f, 0.f);
+    const float2 xyi = make_float2(xi.x, xi.y);
     walk([&](float r2) { return r2 <= P.h2; },
          [&](int k) {
              const float4 xj = X[k];
-             const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+             const float2 rxy = sub_f32x2(xyi, make_float2(xj.x, xj.y));
+             const float rx = rxy.x, ry = rxy.y, rz = xi.z - xj.z;
              const float r2 = rx * rx + ry * ry + rz * rz;
              rho += poly6_in(P, r2);
              if (r2 >= 1e-10f) {
                  const float sc = spiky_scale(P, r2);
-                 const float ax = rx * sc, ay = ry * sc, az = rz * sc;
+                 const float2 axy = mul_f32x2(rxy, sc);
+                 const float ax = axy.x, ay = axy.y, az = rz * sc;
                  sg += (ax * ax + ay * ay + az * az) * P.inv_rho0_sq;
-                 gx += ax;
-                 gy += ay;
+                 gxy = add_f32x2(gxy, axy);
                  gz += az;
              }
          });
+    float gx = gxy.x, gy = gxy.y;
     gx *= P.inv_rho0;
     gy *= P.inv_rho0;
     gz *= P.inv_rho0;
@@ -176,20 +180,23 @@ __device__ __forceinline__ float4 deltap_core(const DevParams& P, const SdfDev& 
                                               float3& dp_raw)
 {
     const float li = xi.w;
-    float dx = 0.f, dy = 0.f, dz = 0.f;
+    float dz = 0.f;
+    float2 dxy = make_float2(0.f, 0.f);
+    const float2 xyi = make_float2(xi.x, xi.y);
     walk([&](float r2) { return r2 <= P.h2 && r2 >= 1e-10f; },
          [&](int k) {
              const float4 xj = X[k];
-             const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+             const float2 rxy = sub_f32x2(xyi, make_float2(xj.x, xj.y));
+             const float rx = rxy.x, ry = rxy.y, rz = xi.z - xj.z;
              const float r2 = rx * rx + ry * ry + rz * rz;
              const float sc = spiky_scale(P, r2);
              float f = li + xj.w;
              if (P.scorr) f += scorr_term(P, r2);
              const float g = sc * f;
-             dx += rx * g;
-             dy += ry * g;
-             dz += rz * g;
+             dxy = fma_f32x2(rxy, g, dxy);
+             dz = __fmaf_rn(rz, g, dz);
          });
+    float dx = dxy.x, dy = dxy.y;
     // rounded products (not fused into the x + dp below)
     dx = __fmul_rn(dx, P.inv_rho0);
     dy = __fmul_rn(dy, P.inv_rho0);
@@ -334,17 +341,20 @@ template <class XS, class MS, class Walk>
 __device__ __forceinline__ bool vorticity_core(const DevParams& P, XS X, MS OMAG, float4 xi, float4 w, Walk&& walk,
                                                float3& dv)
 {
-    float ex = 0.f, ey = 0.f, ez = 0.f;
+    float ez = 0.f;
+    float2 exy = make_float2(0.f, 0.f);
+    const float2 xyi = make_float2(xi.x, xi.y);
     walk([&](float r2) { return r2 <= P.h2 && r2 >= 1e-10f; },
          [&](int k) {
              const float4 xj = X[k];
-             const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+             const float2 rxy = sub_f32x2(xyi, make_float2(xj.x, xj.y));
+             const float rx = rxy.x, ry = rxy.y, rz = xi.z - xj.z;
              const float r2 = rx * rx + ry * ry + rz * rz;
              const float sc = spiky_scale(P, r2) * OMAG[k];
-             ex += rx * sc;
-             ey += ry * sc;
-             ez += rz * sc;
+             exy = fma_f32x2(rxy, sc, exy);
+             ez = __fmaf_rn(rz, sc, ez);
          });
+    float ex = exy.x, ey = exy.y;
     ex *= P.inv_rho0;
     ey *= P.inv_rho0;
     ez *= P.inv_rho0;

@@ -109,6 +109,51 @@ __device__ __forceinline__ float poly6_in(const DevParams& P, float r2)
     return P.poly6 * d * d * d;
 }
 
+// Packed FP32 pairs (sm_100 f32x2 instructions): each lane is rounded exactly
+// as the scalar operation, so a pair computed this way has the scalar bits.
+__device__ __forceinline__ uint64_t f32x2_pack(float2 a)
+{
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+    return r;
+}
+__device__ __forceinline__ float2 f32x2_unpack(uint64_t r)
+{
+    float2 o;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(o.x), "=f"(o.y) : "l"(r));
+    return o;
+}
+// a - b
+__device__ __forceinline__ float2 sub_f32x2(float2 a, float2 b)
+{
+    uint64_t r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f32x2_pack(a)), "l"(f32x2_pack(b)));
+    return f32x2_unpack(r);
+}
+// a + b
+__device__ __forceinline__ float2 add_f32x2(float2 a, float2 b)
+{
+    uint64_t r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f32x2_pack(a)), "l"(f32x2_pack(b)));
+    return f32x2_unpack(r);
+}
+// a * s
+__device__ __forceinline__ float2 mul_f32x2(float2 a, float s)
+{
+    uint64_t r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f32x2_pack(a)), "l"(f32x2_pack(make_float2(s, s))));
+    return f32x2_unpack(r);
+}
+// a * s + c, fused
+__device__ __forceinline__ float2 fma_f32x2(float2 a, float s, float2 c)
+{
+    uint64_t r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;"
+        : "=l"(r)
+        : "l"(f32x2_pack(a)), "l"(f32x2_pack(make_float2(s, s))), "l"(f32x2_pack(c)));
+    return f32x2_unpack(r);
+}
+
 // spiky gradient scalar factor (CS_ComputeLambdas.glsl:83-92): grad = r * s,
 // valid for 1e-10 <= r2 <= h2.  -spiky (h - |r|)^2 / |r| evaluated with one
 // reciprocal square root (|r| = r2 * rsqrt(r2)) instead of a square root and
