@@ -241,24 +241,28 @@ __device__ __forceinline__ void integrate_core(const DevParams& P, const float* 
                                                const SdfDev& sdf, XS X, VS V, float4 x4, float4 v0, float4 p0,
                                                Walk&& walk, float4& xo, float4& vo, float4& omega4)
 {
-    float fx = 0.f, fy = 0.f, fz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+    float fz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+    float2 fxy = make_float2(0.f, 0.f);
+    const float2 xyi = make_float2(x4.x, x4.y), vxy0 = make_float2(v0.x, v0.y);
     if (P.visc_on || P.vort_on) {
         walk([&](float r2) { return r2 <= P.h2; },
              [&](int k) {
                  const float4 xj = X[k];
-                 const float rx = x4.x - xj.x, ry = x4.y - xj.y, rz = x4.z - xj.z;
+                 const float2 rxy = sub_f32x2(xyi, make_float2(xj.x, xj.y));
+                 const float rx = rxy.x, ry = rxy.y, rz = x4.z - xj.z;
                  const float r2 = rx * rx + ry * ry + rz * rz;
                  const float4 vj = V[k];
-                 const float ux = vj.x - v0.x, uy = vj.y - v0.y, uz = vj.z - v0.z;
+                 const float2 uxy = sub_f32x2(make_float2(vj.x, vj.y), vxy0);
+                 const float ux = uxy.x, uy = uxy.y, uz = vj.z - v0.z;
                  if (P.visc_on) {
                      const float w = poly6_in(P, r2) * P.inv_rho0;
-                     fx += ux * w;
-                     fy += uy * w;
-                     fz += uz * w;
+                     fxy = fma_f32x2(uxy, w, fxy);
+                     fz = __fmaf_rn(uz, w, fz);
                  }
                  if (P.vort_on && r2 >= 1e-10f) {
                      const float sc = spiky_scale(P, r2);
-                     const float ax = rx * sc, ay = ry * sc, az = rz * sc;
+                     const float2 axy = mul_f32x2(rxy, sc);
+                     const float ax = axy.x, ay = axy.y, az = rz * sc;
                      // a*b - c*d with the rounding fixed (one product rounded,
                      // one fused), so every instantiation gives the same bits
                      cx += __fmaf_rn(uy, az, -__fmul_rn(uz, ay));
@@ -267,6 +271,7 @@ __device__ __forceinline__ void integrate_core(const DevParams& P, const float* 
                  }
              });
     }
+    const float fx = fxy.x, fy = fxy.y;
     float3 x = make_float3(x4.x, x4.y, x4.z);
     float vdx = 0.f, vdy = 0.f, vdz = 0.f;
     if (P.visc_on) {
