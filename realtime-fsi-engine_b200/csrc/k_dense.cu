@@ -428,7 +428,9 @@ struct RunWalkList {
                         m &= m - 1u;
                         const int k = k0 + c;
                         const float4 xj = __ldg(X + k);
-                        const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+                        // (the pair body repeats this subtraction; the two merge)
+                        const float2 rxy = sub_f32x2(make_float2(xi.x, xi.y), make_float2(xj.x, xj.y));
+                        const float rx = rxy.x, ry = rxy.y, rz = xi.z - xj.z;
                         if (hit(rx * rx + ry * ry + rz * rz)) body(k);
                     }
                 }
