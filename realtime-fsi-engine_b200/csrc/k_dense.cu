@@ -578,6 +578,24 @@ __device__ __forceinline__ void check_drift(const DevParams& P, const DenseArgs&
                      D.gy0, D.gz0, D.nx, D.ny, D.nz);
 }
 
+// Label t moved in the integrate pass: the queries whose runs hold it (the 27
+// window cells around its label's slot) must walk, not replay, in the
+// vorticity pass.
+__device__ __forceinline__ void mark_moved(const DevParams& P, const DenseArgs& D, int t)
+{
+    const float4 b = __ldg(D.xb + t);
+    const int ux = (int)wrap_axis(cell_coord(b.x, P.h), D.gx0, D.nx);
+    const int uy = (int)wrap_axis(cell_coord(b.y, P.h), D.gy0, D.ny);
+    const int uz = (int)wrap_axis(cell_coord(b.z, P.h), D.gz0, D.nz);
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int x = ux + dx, y = uy + dy, z = uz + dz;
+                if (x >= 0 && x < (int)D.nx && y >= 0 && y < (int)D.ny && z >= 0 && z < (int)D.nz)
+                    D.vmark[D.slot0 + ((uint32_t)z * D.ny + (uint32_t)y) * D.nx + (uint32_t)x] = 1;
+            }
+}
+
 // ---- thread order by current cell ----------------------------------------------------------
 // The labels follow the predict-time cells; once the corrections have moved
 // particles, consecutive labels query different current cells and a warp's
@@ -792,7 +810,7 @@ __global__ void __launch_bounds__(kDThreads, 10) k_d_deltap(DevParams P0, DenseA
     });
 }
 
-template <bool B>
+template <bool B, bool R>
 __global__ void __launch_bounds__(kDThreads, 10) k_d_integrate(DevParams P0, DenseArgs D0, const float4* __restrict__ lx,
                                                            const float4* __restrict__ lv, float4* __restrict__ lx0,
                                                            float4* __restrict__ lom,
@@ -809,9 +827,31 @@ __global__ void __launch_bounds__(kDThreads, 10) k_d_integrate(DevParams P0, Den
             const float4 v0 = __ldg(lv + t);
             const float4 p0 = lx0[t];
             float4 vo, om;
-            with_dense_walker(P, D, lx, x4, t, [&](auto&& walk) {
+            auto core = [&](auto&& walk) {
                 integrate_core(P, P.bmin, P.bmax, P.sdf, GSrc{lx}, GSrc{lv}, x4, v0, p0, walk, xo, vo, om);
-            });
+            };
+            if constexpr (R) {
+                // the vorticity pass walks the committed positions, equal to
+                // x* unless the walls or the SDF moved the particle: record
+                // the hit masks, and where a particle moved, mark the query
+                // cells whose runs hold it
+                const int s0 = fast_slot(P, D, x4);
+                if (s0 >= 0) {
+                    int q = 0;
+                    core(RunWalkRec{D.runs, lx, x4, t, s0, (int)D.nx, (int)(D.nx * D.ny), D.hm, P.n, &q});
+                    D.hcnt[t] = q <= kListChunks ? (uint8_t)q : kNoList;
+                } else {
+                    count_bucket_walk(D);
+                    core(BucketWalkLabels{P, D.htable, D.inv, lx, x4, t});
+                    D.hcnt[t] = kNoList;
+                }
+                if (xo.x != x4.x || xo.y != x4.y || xo.z != x4.z) {
+                    D.hcnt[t] = kNoList;
+                    mark_moved(P, D, t);
+                }
+            } else {
+                with_dense_walker(P, D, lx, x4, t, core);
+            }
             if (P.vort_on) lom[t] = om;
             const uint32_t id = __ldg(lid + t);
             pos[id] = xo;
@@ -835,9 +875,13 @@ __global__ void __launch_bounds__(kDThreads, 12) k_d_vorticity(DevParams P0, Den
         const float4 xi = __ldg(lx0 + t);
         float3 dv;
         bool any = false;
-        with_dense_walker(P, D, lx0, xi, t, [&](auto&& walk) {
-            any = vorticity_core(P, GSrc{lx0}, GMag{lom}, xi, __ldg(lom + t), walk, dv);
-        });
+        auto core = [&](auto&& walk) { any = vorticity_core(P, GSrc{lx0}, GMag{lom}, xi, __ldg(lom + t), walk, dv); };
+        const int s0 = D.use_list && __ldg(D.hcnt + t) != kNoList ? interior_slot(P, D, xi) : -1;
+        if (s0 >= 0 && !D.vmark[s0])
+            // integrate walked this particle's runs over the same positions
+            core(RunWalkList{D.runs, lx0, xi, t, s0, (int)D.nx, (int)(D.nx * D.ny), D.hm, P.n});
+        else
+            with_dense_walker(P, D, lx0, xi, t, core);
         if (!any) return;
         const uint32_t id = __ldg(lid + t);
         float4 v = vel[id];
@@ -927,7 +971,18 @@ void launch_d_deltap(const DevParams& P, const DenseArgs& D, const float4* lx_in
 void launch_d_integrate(const DevParams& P, const DenseArgs& D, const float4* lx, const float4* lv, float4* lx0,
                         float4* lom, const uint32_t* lid, float4* pos, float4* vel, cudaStream_t st)
 {
-    PBF_DENSE_LAUNCH(k_d_integrate, dgrid(P.n), kDThreads, P, D, lx, lv, lx0, lom, lid, pos, vel);
+    // R: record hit masks for the vorticity pass
+    if (D.rec_list) {
+        if (D.scenes)
+            k_d_integrate<true, true><<<dgrid(P.n), kDThreads, 0, st>>>(P, D, lx, lv, lx0, lom, lid, pos, vel);
+        else
+            k_d_integrate<false, true><<<dgrid(P.n), kDThreads, 0, st>>>(P, D, lx, lv, lx0, lom, lid, pos, vel);
+    } else {
+        if (D.scenes)
+            k_d_integrate<true, false><<<dgrid(P.n), kDThreads, 0, st>>>(P, D, lx, lv, lx0, lom, lid, pos, vel);
+        else
+            k_d_integrate<false, false><<<dgrid(P.n), kDThreads, 0, st>>>(P, D, lx, lv, lx0, lom, lid, pos, vel);
+    }
 }
 
 void launch_d_vorticity(const DevParams& P, const DenseArgs& D, const float4* lx0, const float4* lom,

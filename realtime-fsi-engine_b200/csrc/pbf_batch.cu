@@ -267,7 +267,7 @@ void pbf_batch::dense_free()
 {
     bfree(lx[0]); bfree(lx[1]); bfree(lxb); bfree(lv); bfree(lx0); bfree(lom); bfree(lrho);
     bfree(lid); bfree(lkey); bfree(inv); bfree(dtable); bfree(druns); bfree(dclean); bfree(ddcol);
-    bfree(ddirty); bfree(dhcnt); bfree(dslot_scene); bfree(dflag); bfree(dslot); bfree(dord); bfree(dcnt);
+    bfree(ddirty); bfree(dhcnt); bfree(dvmark); bfree(dslot_scene); bfree(dflag); bfree(dslot); bfree(dord); bfree(dcnt);
     bfree(dbsum); bfree(dhm);
     dense_ready = false;
 }
@@ -293,7 +293,7 @@ int pbf_batch::dense_setup()
         }
     }
     if ((rc = balloc(dtable, T)) || (rc = balloc(druns, T)) || (rc = balloc(dclean, T)) || (rc = balloc(ddcol, T)) ||
-        (rc = balloc(ddirty, T)) || (rc = balloc(dslot_scene, T)) || (rc = balloc(dcnt, T + 1)) ||
+        (rc = balloc(ddirty, T)) || (rc = balloc(dvmark, T)) || (rc = balloc(dslot_scene, T)) || (rc = balloc(dcnt, T + 1)) ||
         (rc = balloc(dbsum, order_scan_blocks((uint32_t)T)))) {
         dense_free();
         return rc;
@@ -327,6 +327,7 @@ DenseArgs pbf_batch::dense_args() const
     D.clean = dclean;
     D.dcol = ddcol;
     D.dirty = ddirty;
+    D.vmark = dvmark;
     D.htable = table;
     D.inv = inv;
     D.xb = lxb;
@@ -401,13 +402,18 @@ int pbf_batch::dense_step_body()
         order_recorded();
         if (last && vort) {
             if (const int rc = record()) return rc;
+            // hit masks for the vorticity pass
+            BCK(cudaMemsetAsync(dvmark, 0, (size_t)T, stream));
+            D.rec_list = 1;
         }
         launch_d_integrate(P, D, lx[0], lv, lx0, lom, lid, pos, vel, stream);
+        D.rec_list = 0;
         ++launches;
     }
     if (vort) {
         D.rec_slot = nullptr;
         D.rec_cnt = nullptr;
+        D.use_list = 1;
         order_recorded();
         launch_d_vorticity(P, D, lx0, lom, lid, vel, stream);
         ++launches;

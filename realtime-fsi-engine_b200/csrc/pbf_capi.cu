@@ -318,7 +318,7 @@ pbf_handle::~pbf_handle()
     dfree(lx[0]); dfree(lx[1]); dfree(lxb); dfree(lv); dfree(lx0); dfree(lom); dfree(lrho);
     dfree(lid); dfree(lkey); dfree(inv); dfree(list); dfree(lcnt); dfree(lstats); dfree(fastb);
     dfree(dtable); dfree(druns); dfree(dclean); dfree(ddcol); dfree(ddirty); dfree(dflag);
-    dfree(dslot); dfree(dord); dfree(dcnt); dfree(dbsum); dfree(dhm); dfree(dhcnt);
+    dfree(dslot); dfree(dord); dfree(dcnt); dfree(dbsum); dfree(dhm); dfree(dhcnt); dfree(dvmark);
     dfree(grid); dfree(slab_min);
     mesh_free();
     if (stream) cudaStreamDestroy(stream);
@@ -448,6 +448,8 @@ DenseArgs pbf_handle::dense_args() const
     D.clean = dclean;
     D.dcol = ddcol;
     D.dirty = ddirty;
+    D.rec_list = 0;
+    D.vmark = dvmark;
     D.htable = table;
     D.inv = inv;
     D.xb = lxb;
@@ -495,7 +497,7 @@ int pbf_handle::ensure_dense()
         if ((rc = dalloc(dtable, slots)) || (rc = dalloc(druns, slots)) || (rc = dalloc(dcnt, slots + 1)) ||
             (rc = dalloc(dbsum, order_scan_blocks((uint32_t)slots))) || (rc = dalloc(dclean, slots)) ||
             (rc = dalloc(ddcol, slots)) ||
-            (rc = dalloc(ddirty, slots)))
+            (rc = dalloc(ddirty, slots)) || (rc = dalloc(dvmark, slots)))
             return rc;
         cap_slots = slots;
     }
@@ -661,12 +663,18 @@ int pbf_handle::stage(int st, uint32_t iter)
             dlist_iter = 0;
             if (P.vort_on) {
                 if (const int rc = record_next()) return rc;
+                // hit masks for the vorticity pass
+                CK(cudaMemsetAsync(dvmark, 0, slots, stream));
+                D.rec_list = 1;
+                dvlist_ready = true;
             }
             launch_d_integrate(P, D, lx[0], lv, lx0, lom, lid, pos, vel, stream);
             break;
         default:
             order_by(lx0);
             dord_iter = 0;
+            D.use_list = dvlist_ready ? 1 : 0;
+            dvlist_ready = false;
             launch_d_vorticity(P, D, lx0, lom, lid, vel, stream);
             break;
         }
@@ -722,6 +730,7 @@ int pbf_handle::stage(int st, uint32_t iter)
             CK(cudaMemsetAsync(ddirty, 0, slots, stream));
             dord_iter = 0;
             dlist_iter = 0;
+            dvlist_ready = false;
             dslot_fresh = false;
             CK(cudaMemsetAsync(dflag, 0, sizeof(uint32_t), stream));
             label_space = true;

@@ -79,6 +79,8 @@ struct pbf_handle {
     uint32_t* dhm = nullptr;
     uint8_t* dhcnt = nullptr;
     int dlist_iter = 0;          // solver iteration whose lambda recorded them (0: none)
+    uint8_t* dvmark = nullptr;   // per window slot: integrate moved a particle its runs hold
+    bool dvlist_ready = false;   // dhm/dhcnt hold the integrate pass's masks for the vorticity pass
     size_t cap_slots = 0;
     int dwin_g0[3] = {0, 0, 0};
     uint32_t dwin_n[3] = {0, 0, 0};

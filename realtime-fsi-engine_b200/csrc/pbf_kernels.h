@@ -148,6 +148,8 @@ struct DenseArgs {
     uint32_t* hm;          // lambda hit masks for the delta-p of the same iteration (kDenseListWords x n)
     uint8_t* hcnt;         // per label: chunks recorded, 0xFF = none
     int use_list;          // delta-p: the lambda pass of this iteration recorded hm/hcnt
+    int rec_list;          // integrate: record hm/hcnt for the vorticity pass (positions it leaves in place)
+    uint8_t* vmark;        // per window slot: a query there sees a particle integrate moved (no replay)
     uint32_t* rec_slot;    // delta-p / integrate (may be null): current slot of each output position
     uint32_t* rec_cnt;     //   and per-slot counts (zeroed by the caller), for the next pass's order
     const uint8_t* clean;  // per window slot: 1 = no hash collision near the cell
