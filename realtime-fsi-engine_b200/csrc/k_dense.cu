@@ -124,6 +124,55 @@ __global__ void __launch_bounds__(256) k_d_keys(DevParams P0, DenseArgs D0, cons
     }
 }
 
+// The same keys straight from the particle state: x* re-derived from
+// (pos, vel) of particle ids[s] exactly as the predict pass derives it.
+template <bool B>
+__global__ void __launch_bounds__(256) k_d_keys_pred(DevParams P0, DenseArgs D0, const uint32_t* __restrict__ ids,
+                                                     const float4* __restrict__ pos, const float4* __restrict__ vel,
+                                                     uint32_t* __restrict__ dkey)
+{
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < P0.n; s += stride) {
+        const uint32_t id = __ldg(ids + s);
+        float3 vp, xs;
+        predict_particle(P0, __ldg(pos + id), __ldg(vel + id), vp, xs);
+        with_scene<B>(P0, D0, (int)s, [&](const DevParams& P, const DenseArgs& D) {
+            dkey[s] = dense_key(D, cell_coord(xs.x, P.h), cell_coord(xs.y, P.h), cell_coord(xs.z, P.h));
+        });
+    }
+}
+
+// Label t = hash-sorted index order[t]: its x* (also the predict-time copy),
+// predicted velocity, substep-start position, id and key, gathered from the
+// particle state (the predict pass's arithmetic again), and inv[order[t]] = t.
+__global__ void __launch_bounds__(256) k_d_permute(DevParams P, const uint32_t* __restrict__ order,
+                                                   const uint32_t* __restrict__ ids,
+                                                   const uint32_t* __restrict__ skeys,
+                                                   const float4* __restrict__ pos, const float4* __restrict__ vel,
+                                                   float4* __restrict__ lx, float4* __restrict__ lxb,
+                                                   float4* __restrict__ lv, float4* __restrict__ lx0,
+                                                   uint32_t* __restrict__ lid, uint32_t* __restrict__ lkey,
+                                                   uint32_t* __restrict__ inv)
+{
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < P.n; t += stride) {
+        const uint32_t s = __ldg(order + t);
+        const uint32_t id = __ldg(ids + s);
+        const float4 p = __ldg(pos + id);
+        const float4 v = __ldg(vel + id);
+        float3 vp, xs;
+        predict_particle(P, p, v, vp, xs);
+        const float4 x = make_float4(xs.x, xs.y, xs.z, 0.0f);
+        lx[t] = x;
+        lxb[t] = x;
+        lv[t] = make_float4(vp.x, vp.y, vp.z, v.w);
+        lx0[t] = p;
+        lid[t] = id;
+        lkey[t] = __ldg(skeys + s);
+        inv[s] = t;
+    }
+}
+
 // The window of global slot g (its scene's, in a batch) and g's slot in it.
 template <bool B>
 __device__ __forceinline__ uint32_t window_of_slot(DenseArgs& D, uint32_t& mask, uint32_t g)
@@ -912,6 +961,20 @@ static inline unsigned capped_grid(uint32_t n, uint32_t threads, int sms, uint32
 void launch_d_keys(const DevParams& P, const DenseArgs& D, const float4* sx, uint32_t* dkey, int sms, cudaStream_t st)
 {
     PBF_DENSE_LAUNCH(k_d_keys, capped_grid(P.n, 256, sms, 8), 256, P, D, sx, dkey);
+}
+
+void launch_d_keys_pred(const DevParams& P, const DenseArgs& D, const uint32_t* ids, const float4* pos,
+                        const float4* vel, uint32_t* dkey, int sms, cudaStream_t st)
+{
+    PBF_DENSE_LAUNCH(k_d_keys_pred, capped_grid(P.n, 256, sms, 8), 256, P, D, ids, pos, vel, dkey);
+}
+
+void launch_d_permute(const DevParams& P, const uint32_t* order, const uint32_t* ids, const uint32_t* skeys,
+                      const float4* pos, const float4* vel, float4* lx, float4* lxb, float4* lv, float4* lx0,
+                      uint32_t* lid, uint32_t* lkey, uint32_t* inv, int sms, cudaStream_t st)
+{
+    k_d_permute<<<capped_grid(P.n, 256, sms, 8), 256, 0, st>>>(P, order, ids, skeys, pos, vel, lx, lxb, lv, lx0, lid,
+                                                               lkey, inv);
 }
 
 void launch_d_clean(const DenseArgs& D, uint32_t mask, uint8_t* clean, uint32_t* unclean, int sms, cudaStream_t st)

@@ -371,14 +371,13 @@ int pbf_batch::dense_step_body()
         launch_radix_sort(n, key_bits, keys, ka, ia, kb, ib, hist, totals, &skeys, &ids, stream, &launches);
         BCK(cudaMemsetAsync(table, 0xFF, sizeof(int2) * (size_t)table_size, stream));
         launch_build_table(n, skeys, table, sms, stream);
-        launch_b_reorder(P, scenes_dev, scene_of, ids, pos, vel, sx[0], sv, sx0, lod, nullptr, mbits, sms, stream);
         D = dense_args();
-        launch_d_keys(P, D, sx[0], mcode, sms, stream);
-        launches += 4;
+        launch_d_keys_pred(P, D, ids, pos, vel, mcode, sms, stream);
+        launches += 3;
         uint32_t *msorted = nullptr, *lorder = nullptr;
         launch_radix_sort(n, slot_bits, mcode, mka, mia, mkb, mib, hist, totals, &msorted, &lorder, stream,
                           &launches);
-        launch_l_permute(n, lorder, ids, skeys, sx[0], sv, sx0, lx[0], lxb, lv, lx0, lid, lkey, inv, sms, stream);
+        launch_d_permute(P, lorder, ids, skeys, pos, vel, lx[0], lxb, lv, lx0, lid, lkey, inv, sms, stream);
         BCK(cudaMemsetAsync(dtable, 0xFF, sizeof(int2) * (size_t)T, stream));
         launch_build_table(n, msorted, dtable, sms, stream);
         launch_d_runs(D, dtable, druns, sms, stream);

@@ -548,7 +548,7 @@ ListArgs pbf_handle::list_args() const
     return A;
 }
 
-// Sorted-order buffers are kept in label order in mode 6: gather the one
+// Sorted-order buffers are kept in label order in modes 6 and 8: gather the one
 // asked for back into sorted (hash) order before it is read.
 int pbf_handle::unpermute_for_read(int which)
 {
@@ -562,6 +562,9 @@ int pbf_handle::unpermute_for_read(int which)
         break;
     case PBF_BUF_OMEGA:
         launch_l_unpermute4(n, inv, lom, somega, num_sms, stream);
+        break;
+    case PBF_BUF_VPRED:
+        launch_l_unpermute4(n, inv, lv, sv, num_sms, stream);
         break;
     default:
         return PBF_OK;
@@ -706,22 +709,22 @@ int pbf_handle::stage(int st, uint32_t iter)
         break;
     case PBF_STAGE_REORDER:
         prof_begin(PBF_STAGE_REORDER);
-        launch_reorder(P, ids, pos, vel, sx[0], sv, sx0, lod, mode && mode != 8 ? mcode : nullptr, sms, stream);
-        ++launches;
         order = nullptr;
         if (mode == 8) {
-            // relabel by window slot, then the slot table of the labels
+            // relabel by window slot, then the slot table of the labels (the
+            // hash-sorted arrays are not needed: keys and label-order arrays
+            // come straight from the particle state)
             int rc = ensure_dense();
             if (rc) return rc;
             const DenseArgs D = dense_args();
-            launch_d_keys(P, D, sx[0], mcode, sms, stream);
+            launch_d_keys_pred(P, D, ids, pos, vel, mcode, sms, stream);
             ++launches;
             const uint64_t slots = (uint64_t)dwin_n[0] * dwin_n[1] * dwin_n[2];
             uint32_t bits = 1;
             while ((1ull << bits) < slots) ++bits;
             uint32_t* msorted = nullptr;
             launch_radix_sort(n, bits, mcode, mka, mia, mkb, mib, hist, totals, &msorted, &order, stream, &launches);
-            launch_l_permute(n, order, ids, skeys, sx[0], sv, sx0, lx[0], lxb, lv, lx0, lid, lkey, inv, sms, stream);
+            launch_d_permute(P, order, ids, skeys, pos, vel, lx[0], lxb, lv, lx0, lid, lkey, inv, sms, stream);
             ++launches;
             CK(cudaMemsetAsync(dtable, 0xFF, sizeof(int2) * slots, stream));
             launch_build_table(n, msorted, dtable, sms, stream);
@@ -738,6 +741,8 @@ int pbf_handle::stage(int st, uint32_t iter)
             prof_end(PBF_STAGE_REORDER);
             break;
         }
+        launch_reorder(P, ids, pos, vel, sx[0], sv, sx0, lod, mode ? mcode : nullptr, sms, stream);
+        ++launches;
         if (mode) {
             uint32_t* msorted = nullptr;
             launch_radix_sort(n, 24, mcode, mka, mia, mkb, mib, hist, totals, &msorted, &order, stream, &launches);

@@ -169,6 +169,13 @@ struct DenseArgs {
     const uint16_t* slot_scene;  // batch: scene of each global slot
 };
 void launch_d_keys(const DevParams& P, const DenseArgs& D, const float4* sx, uint32_t* dkey, int sms, cudaStream_t st);
+// The keys and the label-order gather straight from (pos, vel) of the
+// hash-sorted ids, re-deriving x* and v' as the predict pass does.
+void launch_d_keys_pred(const DevParams& P, const DenseArgs& D, const uint32_t* ids, const float4* pos,
+                        const float4* vel, uint32_t* dkey, int sms, cudaStream_t st);
+void launch_d_permute(const DevParams& P, const uint32_t* order, const uint32_t* ids, const uint32_t* skeys,
+                      const float4* pos, const float4* vel, float4* lx, float4* lxb, float4* lv, float4* lx0,
+                      uint32_t* lid, uint32_t* lkey, uint32_t* inv, int sms, cudaStream_t st);
 void launch_d_clean(const DenseArgs& D, uint32_t mask, uint8_t* clean, uint32_t* unclean, int sms, cudaStream_t st);
 void launch_d_dcol(const DenseArgs& D, uint32_t mask, uint8_t* dcol, int sms, cudaStream_t st);
 void launch_d_runs(const DenseArgs& D, const int2* cells, int2* runs, int sms, cudaStream_t st);
