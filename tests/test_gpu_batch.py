@@ -129,6 +129,23 @@ def test_dense_windows_with_hash_collisions(have_gpu):
     assert np.array_equal(got["pos"], base["pos"]) and np.array_equal(got["vel"], base["vel"])
 
 
+def test_dense_windows_with_drift_marks(have_gpu):
+    """Particles placed 1.5 h beyond a wall are clamped back by more than the
+    0.9 h drift bound; with small hash tables the queries they can reach
+    through a colliding bucket are marked and walk the buckets for the rest
+    of the substep: still the bits of the hashed-bucket walk."""
+    cfg, sc = small_c3()
+    for k, s in enumerate(sc):
+        s["hash_size"] = 4096
+        pos = s["pos"].copy()
+        m = min(50, len(pos))
+        pos[:m, 0] = s["bounds_max"][0] + 1.5 * cfg.h
+        s["pos"] = pos
+    base = run_batch(cfg, sc, 2, [(P.BOPT_NEIGHBOUR_MODE, 4)])
+    got = run_batch(cfg, sc, 2, [(P.BOPT_NEIGHBOUR_MODE, 8)])
+    assert np.array_equal(got["pos"], base["pos"]) and np.array_equal(got["vel"], base["vel"])
+
+
 def test_dense_windows_match_one_handle_per_scene(have_gpu):
     cfg, sc = small_c3()
     got = run_batch(cfg, sc, 3, [(P.BOPT_NEIGHBOUR_MODE, 8)])
