@@ -38,6 +38,20 @@ def test_struct_layouts():
     assert DerivedParams.w0_self.offset == 108 and DerivedParams.hash_mask.offset == 112
 
 
+def test_batch_option_constants_and_tuning_layout_match_header():
+    """The batch option numbers and pbf_batch_tuning's fields in the Python
+    binding are the header's."""
+    from pbf_b200 import _capi
+    hdr = open(os.path.join(ROOT, "include", "pbf_b200.h")).read()
+    for name in ("BLOCK", "ORDER", "BLOCKS_PER_SM", "USE_GRAPH", "NEIGHBOUR_MODE"):
+        m = re.search(r"#define PBF_BOPT_%s (\d+)" % name, hdr)
+        assert m and int(m.group(1)) == getattr(_capi, "BOPT_" + name), name
+    body = re.search(r"typedef struct pbf_batch_tuning \{(.*?)\} pbf_batch_tuning;", hdr, re.S).group(1)
+    fields = re.findall(r"(?:int32_t|float) (\w+);", body)
+    assert fields == [f[0] for f in _capi.BatchTuning._fields_]
+    assert C.sizeof(_capi.BatchTuning) == 4 * len(fields)
+
+
 def test_default_config_matches_reference_defaults():
     import pbf_b200 as P
     c = P.default_config()
