@@ -905,7 +905,9 @@ __global__ void __launch_bounds__(kDThreads, 10) k_d_integrate(DevParams P0, Den
             const uint32_t id = __ldg(lid + t);
             pos[id] = xo;
             vel[id] = vo;
-            lx0[t] = xo;
+            // (the committed position carries |omega| in w for the vorticity
+            // pass, which then reads a neighbour's position and |omega| in one load)
+            lx0[t] = P.vort_on ? make_float4(xo.x, xo.y, xo.z, om.w) : xo;
             check_drift(P, D, xo, t);
         }
         if (D.rec_cnt) record_slot(P, D, xo, t, live);
@@ -924,7 +926,7 @@ __global__ void __launch_bounds__(kDThreads, 12) k_d_vorticity(DevParams P0, Den
         const float4 xi = __ldg(lx0 + t);
         float3 dv;
         bool any = false;
-        auto core = [&](auto&& walk) { any = vorticity_core(P, GSrc{lx0}, GMag{lom}, xi, __ldg(lom + t), walk, dv); };
+        auto core = [&](auto&& walk) { any = vorticity_core(P, GSrc{lx0}, GMagX{lx0}, xi, __ldg(lom + t), walk, dv); };
         const int s0 = D.use_list && __ldg(D.hcnt + t) != kNoList ? interior_slot(P, D, xi) : -1;
         if (s0 >= 0 && !D.vmark[s0])
             // integrate walked this particle's runs over the same positions

@@ -78,6 +78,10 @@ struct SSrc {
     const float4* p;
     __device__ __forceinline__ float4 operator[](int k) const { return p[k]; }
 };
+struct GMagX {  // |omega| in the w of a position array, read as the whole float4 the pair body loads anyway
+    const float4* __restrict__ p;
+    __device__ __forceinline__ float operator[](int k) const { return __ldg(p + k).w; }
+};
 struct SMagW {  // |omega| staged in the w of a position array
     const float4* p;
     __device__ __forceinline__ float operator[](int k) const { return p[k].w; }
