@@ -170,6 +170,22 @@ def test_neighbour_mode_option(have_gpu):
         b.set_option(P.BOPT_NEIGHBOUR_MODE, 6)
 
 
+def test_dense_windows_refused_when_too_large(have_gpu):
+    """A scene whose walls span more than 2^26 cells in all has no dense
+    window: mode 8 is refused and the automatic choice walks the buckets."""
+    cfg, sc = small_c3(sizes=[700, 1500])
+    sc[1]["bounds_max"] = (400.0, 400.0, 400.0)  # 10^4 cells per axis at h = 0.04
+    b = PB.make_batch(cfg, sc)
+    with pytest.raises(P.PBFError):
+        b.set_option(P.BOPT_NEIGHBOUR_MODE, 8)
+    for _ in range(2):
+        b.step()
+    b.sync()
+    got = b.read_particles()
+    base = run_batch(cfg, sc, 2, [(P.BOPT_NEIGHBOUR_MODE, 4)])
+    assert np.array_equal(got["pos"], base["pos"]) and np.array_equal(got["vel"], base["vel"])
+
+
 def test_per_scene_io_and_errors(have_gpu):
     cfg, sc = small_c3()
     b = PB.make_batch(cfg, sc)
