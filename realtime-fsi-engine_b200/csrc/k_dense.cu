@@ -110,22 +110,8 @@ __device__ __forceinline__ uint32_t dense_key(const DenseArgs& D, int cx, int cy
            (wrap_axis(cz, D.gz0, D.nz) * D.ny + wrap_axis(cy, D.gy0, D.ny)) * D.nx + wrap_axis(cx, D.gx0, D.nx);
 }
 
-// Window slot of each hash-sorted particle's predict-time cell.
-template <bool B>
-__global__ void __launch_bounds__(256) k_d_keys(DevParams P0, DenseArgs D0, const float4* __restrict__ sx,
-                                                uint32_t* __restrict__ dkey)
-{
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < P0.n; s += stride) {
-        with_scene<B>(P0, D0, (int)s, [&](const DevParams& P, const DenseArgs& D) {
-            const float4 x = __ldg(sx + s);
-            dkey[s] = dense_key(D, cell_coord(x.x, P.h), cell_coord(x.y, P.h), cell_coord(x.z, P.h));
-        });
-    }
-}
-
-// The same keys straight from the particle state: x* re-derived from
-// (pos, vel) of particle ids[s] exactly as the predict pass derives it.
+// Window slot of each hash-sorted particle's predict-time cell, x* re-derived
+// from (pos, vel) of particle ids[s] exactly as the predict pass derives it.
 template <bool B>
 __global__ void __launch_bounds__(256) k_d_keys_pred(DevParams P0, DenseArgs D0, const uint32_t* __restrict__ ids,
                                                      const float4* __restrict__ pos, const float4* __restrict__ vel,
@@ -279,10 +265,9 @@ __global__ void __launch_bounds__(128) k_d_dcol(DenseArgs D0, uint32_t mask0, ui
     }
 }
 
-// Candidates lo .. hi-1 of one run in chunks of kChunk, tested into a hit
-// mask; the body runs for the hits in candidate order (masked_walk's scheme).
-// map(k) gives the label of candidate k (identity for a run; the hash-slot
-// -> label map for a bucket).
+// Candidates lo .. hi-1 of one hashed bucket in chunks of kChunk, tested into
+// a hit mask; the body runs for the hits in candidate order (masked_walk's
+// scheme).  map(k) gives the label of candidate k (the hash-slot -> label map).
 struct NoRecord {
     __device__ __forceinline__ void operator()(uint32_t) const {}
 };
@@ -354,9 +339,6 @@ __device__ __forceinline__ void label_range(const float4* __restrict__ X, float4
     }
 }
 
-struct IdMap {
-    __device__ __forceinline__ int operator()(int k) const { return k; }
-};
 struct InvMap {
     const uint32_t* __restrict__ inv;
     __device__ __forceinline__ int operator()(int k) const { return (int)__ldg(inv + k); }
@@ -959,11 +941,6 @@ static inline unsigned capped_grid(uint32_t n, uint32_t threads, int sms, uint32
         else                                                                                      \
             KERNEL<false><<<(GRID), (BLOCK), 0, st>>>(__VA_ARGS__);                               \
     } while (0)
-
-void launch_d_keys(const DevParams& P, const DenseArgs& D, const float4* sx, uint32_t* dkey, int sms, cudaStream_t st)
-{
-    PBF_DENSE_LAUNCH(k_d_keys, capped_grid(P.n, 256, sms, 8), 256, P, D, sx, dkey);
-}
 
 void launch_d_keys_pred(const DevParams& P, const DenseArgs& D, const uint32_t* ids, const float4* pos,
                         const float4* vel, uint32_t* dkey, int sms, cudaStream_t st)

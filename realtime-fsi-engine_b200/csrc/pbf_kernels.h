@@ -168,7 +168,6 @@ struct DenseArgs {
     const uint16_t* scene_of;    // batch: scene of each label / hash-sorted index (scene-contiguous)
     const uint16_t* slot_scene;  // batch: scene of each global slot
 };
-void launch_d_keys(const DevParams& P, const DenseArgs& D, const float4* sx, uint32_t* dkey, int sms, cudaStream_t st);
 // The keys and the label-order gather straight from (pos, vel) of the
 // hash-sorted ids, re-deriving x* and v' as the predict pass does.
 void launch_d_keys_pred(const DevParams& P, const DenseArgs& D, const uint32_t* ids, const float4* pos,
