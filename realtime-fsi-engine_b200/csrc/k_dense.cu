@@ -462,7 +462,11 @@ struct RunWalkList {
                         // (the pair body repeats this subtraction; the two merge)
                         const float2 rxy = sub_f32x2(make_float2(xi.x, xi.y), make_float2(xj.x, xj.y));
                         const float rx = rxy.x, ry = rxy.y, rz = xi.z - xj.z;
-                        if (hit(rx * rx + ry * ry + rz * rz)) body(k);
+                        // a recorded hit passed r^2 <= h^2 with these positions and this
+                        // arithmetic; of the replaying passes' test (r^2 <= h^2 and
+                        // r^2 >= 1e-10, delta-p and vorticity alike) the lower bound remains
+                        (void)hit;
+                        if (rx * rx + ry * ry + rz * rz >= 1e-10f) body(k);
                     }
                 }
             }
