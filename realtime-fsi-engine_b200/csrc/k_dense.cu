@@ -36,10 +36,25 @@
 // particle is whose neighbourhood holds a colliding cell ("dirty" for the rest
 // of the substep): only a query in such a cell can see it through another
 // cell's bucket.  A particle whose cell fails (a), (b) or (c) walks the 27
-// hashed buckets
-// (through the hash-slot -> label map).  Both walks test candidates in chunks
-// into a hit mask exactly as the hashed-bucket passes do, so a pair's
-// arithmetic is the same in every walk.
+// hashed buckets (through the hash-slot -> label map).  Both walks test
+// candidates in chunks into a hit mask and run the shared pair bodies of
+// masked_body.cuh for the hits in candidate order, so a pair's arithmetic is
+// the same in every walk and every mode.
+//
+// Work saved on top of the runs:
+//   * passes after the first iteration take their threads in current-cell
+//     order (a counting sort of the slots the previous pass recorded), so a
+//     warp's lanes walk the same few runs;
+//   * the delta-p pass replays the hit masks its iteration's lambda pass
+//     recorded (same positions, same runs, same hits), and the vorticity pass
+//     those of the integrate pass, except near particles the walls or the
+//     SDF moved there;
+//   * x/y arithmetic in packed f32x2 instructions, each lane rounded as the
+//     scalar operation.
+// One kernel serves one scene (B = false, constants read from the kernel
+// parameters) or a batch (B = true): each scene has its own window at its own
+// offset in one global slot space, and a thread takes its label's scene's hash
+// mask, bucket offset, walls, SDF and window.
 #include "masked_body.cuh"
 #include "pbf_batch.h"
 #include "pbf_kernels.h"
