@@ -10,7 +10,10 @@ iterations, static capsule SDF obstacle (r=0.1, axis z, x=1.2), FP32.  A
 
 Timing: W untimed steps, then exactly K steps between CUDA events recorded on
 the engine's stream, with a barrier + device synchronize on both sides; the
-maximum over ranks is reported.  The working set (~1.7 GB) is far larger than
+maximum over ranks is reported.  Each step replays the CUDA graph of the whole
+step (pbf_set_use_graph); the per-pass times come from the same W + K steps
+run again from the same state, launched one by one with events around every
+pass (pbf_set_profiling).  The working set (~1.7 GB) is far larger than
 the 126 MB L2, so no flush is needed between steps.  For N > 1 every rank steps
 its own replica of the scene (the plain step does not shard; no collective).
 """
@@ -251,11 +254,13 @@ def run_b200(args, dist):
         fl.setSDFPadding(pad)
         fl.setSDFContainment(False)
     stream = torch.cuda.ExternalStream(fl.stream(), device=dev)
+    # timed: each step replays the CUDA graph of the whole step (captured on the
+    # first warm-up step), no per-pass events
+    start = fl.readbackParticles()
+    fl.set_use_graph(True)
     for _ in range(args.warmup):
         fl.step()
     fl.sync()
-    fl.set_profiling(True)
-    fl.reset_pass_times()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     dist.barrier()
     torch.cuda.synchronize(dev)
@@ -274,9 +279,25 @@ def run_b200(args, dist):
     launches = fl.kernel_launches() - l0
     ws1 = fl.list_stats() if ws0 is not None else None
     ms = e0.elapsed_time(e1)
+    bad = fl.check_finite()
+    # per-pass times: the same steps again from the same state, launched one
+    # by one with CUDA events around every pass (the simulation is
+    # deterministic, so the passes see the same particles as the timed run)
+    fl.set_use_graph(False)
+    fl.setParticles(start)
+    for _ in range(args.warmup):
+        fl.step()
+    fl.sync()
+    fl.set_profiling(True)
+    fl.reset_pass_times()
+    for _ in range(args.steps):
+        fl.step()
+    fl.sync()
     passes = fl.pass_times()
     fl.set_profiling(False)
-    bad = fl.check_finite()
+    fl.set_use_graph(True)
+    fl.step()  # re-capture the graph outside the e2e timing
+    fl.sync()
     ms_max = dist.max(ms)
     subs = cfg.substep_iterations
     value = n * subs * args.steps * dist.world / (ms_max / 1e3)
