@@ -34,6 +34,9 @@ class CoupledScene:
                  incremental=True, device=0):
         self.fluid = PBFluids(cfg, device)
         self.fluid.setParticles(make_particles(pos, vel))
+        # the step replays one CUDA graph; refitting the mesh SDF rewrites the
+        # grid in place, which the graph reads without being re-captured
+        self.fluid.set_use_graph(True)
         self.sdf = SDFBoundary(device)
         self.sdf.buildFromMesh(verts, faces, sdf_cell)
         self.fluid.setSDFBoundary(self.sdf)
