@@ -3,7 +3,7 @@
  *
  * This is the drop-in boundary for the fluid-solver hot path of
  * enderenest/Realtime-FSI-Engine.  The reference exposes that path only as the
- * C++ class `PBFluids` (include/fluid/PBFluids.h:191-371) plus the
+ * C++ class `PBFluids` (include/fluid/PBFluids.h:88-163) plus the
  * `SDFBoundary` obstacle (include/fluid/SDFBoundary.h:38-167) and the
  * fluid-to-mesh contact reduction in src/main.cpp:604-710.  Every entry point
  * below names the reference member or function it replaces.  The C++ classes
@@ -259,9 +259,11 @@ int pbf_build_table(const uint32_t* sorted_keys, uint32_t n, uint32_t hash_size,
  * cannot call cudaMalloc (device memory owned by another framework's pool,
  * plugins handed only device buffers, real-time loops that must not enter the
  * allocator).  No counterpart in the reference.  keys_dev, sorted_keys_dev and
- * sorted_ids_dev are caller-owned device arrays of n uint32 (keys must not
- * alias the outputs); the work is queued on `stream` (a cudaStream_t, NULL for
- * the default stream) and the call returns without synchronizing.  Scratch
+ * sorted_ids_dev are caller-owned device arrays of n uint32, no two of which
+ * may overlap (PBF_ERR_INVALID otherwise); the work is queued on `stream` (a
+ * cudaStream_t of the current device, NULL for the default stream; a stream of
+ * another device gives PBF_ERR_INVALID) and the call returns without
+ * synchronizing.  Scratch
  * comes from one fixed device array of the library (about 8.3 MB, kept by
  * every GPU that loads the library until exit), so n is limited to
  * PBF_NOALLOC_MAX_KEYS, and calls whose GPU work overlaps (other streams or
@@ -467,6 +469,51 @@ int pbf_deform_step(pbf_deform* d, const float* forces3, int32_t nv, float dt, c
 int pbf_deform_patch_size(pbf_deform* d, int32_t* size);
 /* Incremental path: max |x - x_dense| on the x axis (-1 if not ready). */
 int pbf_deform_verify_incremental(pbf_deform* d, double* max_diff);
+
+/* ---- scene presets and headless set-up (include/core/Scene.h,
+ *      include/core/SceneSetup.h) --------------------------------------------
+ * Host code, no GPU.  The presets are Scene.h:70-306's four scenes; the
+ * set-up steps are the application's (src/main.cpp): loadOFF :364-415,
+ * fitMeshToDomain :419-432, the fit centre of loadMeshBoundary :500-512,
+ * applyMeshTransform :747-770, spawnParticles :160-188. */
+typedef struct pbf_scene_preset {
+    char name[48];
+    pbf_fluid_config fluid;
+    float cam_yaw, cam_pitch, cam_dist, point_size;
+    char mesh_file[64];          /* asset file name, e.g. "cube1538.off"        */
+    float mesh_fit_size;         /* largest extent after fitting                */
+    float sdf_cell;              /* SDF voxel size                              */
+    float sdf_padding;
+    uint32_t sdf_container;      /* 1: fluid held inside the mesh               */
+    float mesh_translate[3];     /* offset from the fitted pose                 */
+    float mesh_rot_deg[3];       /* degrees about X, Y, Z (Rx * Ry * Rz)        */
+    pbf_deform_params deform;    /* SceneDeform's first seven fields            */
+    int32_t local_kring;         /* SceneDeform::localKRing                     */
+    float contact_radius;        /* SceneDeform::contactRadius                  */
+} pbf_scene_preset;
+
+/* Number of presets (4). */
+int pbf_scene_count(void);
+int pbf_scene_get(int32_t index, pbf_scene_preset* out);
+/* Reads an OFF mesh (comments and blank lines skipped, any *OFF header,
+ * first three numbers of a vertex line, polygons fan-triangulated).  *nv and
+ * *nf always receive the counts; verts3 (nv x 3) and faces3 (nf x 3) are
+ * filled when their capacities (in vertices / triangles) suffice, so a
+ * caller may ask for the counts first with null arrays. */
+int pbf_off_load(const char* path, double* verts3, int32_t vcap, int32_t* faces3, int32_t fcap, int32_t* nv,
+                 int32_t* nf);
+/* Centre the bounding box on center and scale the largest extent to
+ * target_size (in place). */
+int pbf_mesh_fit(double* verts3, int32_t nv, const float center[3], double target_size);
+/* The fit centre a scene uses: walls' middle in x and z, 40 % up in y. */
+int pbf_mesh_fit_center(const pbf_fluid_config* cfg, float center_out[3]);
+/* Rotate about the bounding-box centre (degrees, X then Y then Z) and
+ * translate, in single precision (in place). */
+int pbf_mesh_place(double* verts3, int32_t nv, const float translate[3], const float rot_deg[3]);
+/* The reference's spawner for cfg (lattice, or seeded uniform with
+ * spawn_random).  *count always receives the number of particles; `out` is
+ * filled when capacity suffices. */
+int pbf_spawn_particles(const pbf_fluid_config* cfg, pbf_particle* out, uint32_t capacity, uint32_t* count);
 
 /* ---- differentiable step ----------------------------------------------------
  * No reference counterpart.  Reverse-mode derivative of one step of a batch

@@ -74,7 +74,13 @@ __device__ Hit subtree_closest(const MeshDev& M, float3 P, int root, float bound
     best.face = -1;
     if (M.nf <= 0 || root < 0) return best;
     const int n_int = M.nf - 1;
-    int stack[64];
+    // Depth bound: each internal node splits its range at a strictly longer
+    // common prefix of the 64-bit (Morton code, leaf index) keys than its
+    // parent did, so no path is longer than 64 internal nodes.  A pop pushes
+    // at most two nodes, one of which is popped next, so the stack never holds
+    // more than depth + 2 <= 66 entries and kStack is never reached.
+    constexpr int kStack = 96;
+    int stack[kStack];
     int sp = 0;
     stack[sp++] = root;
     while (sp > 0) {
@@ -102,8 +108,8 @@ __device__ Hit subtree_closest(const MeshDev& M, float3 P, int root, float bound
         // push the farther child first so the nearer one is visited first
         const int nearc = dl <= dr ? ch.x : ch.y, farc = dl <= dr ? ch.y : ch.x;
         const float dnear = fminf(dl, dr), dfar = fmaxf(dl, dr);
-        if (dfar < best.d2 && sp < 64) stack[sp++] = farc;
-        if (dnear < best.d2 && sp < 64) stack[sp++] = nearc;
+        if (dfar < best.d2 && sp < kStack) stack[sp++] = farc;
+        if (dnear < best.d2 && sp < kStack) stack[sp++] = nearc;
     }
     return best;
 }

@@ -19,6 +19,7 @@ namespace pbf {
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
+static_assert(kSortTile == (int)kSortTileKeys, "scratch sizing elsewhere uses kSortTileKeys");
 constexpr int kRadix = 256;
 constexpr int kWarps = kSortThreads / 32;
 

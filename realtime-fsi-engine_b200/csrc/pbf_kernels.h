@@ -195,6 +195,9 @@ void launch_d_vorticity(const DevParams& P, const DenseArgs& D, const float4* lx
                         const uint32_t* lid, float4* vel, cudaStream_t st);
 
 // ---- k_sort.cu ----------------------------------------------------------------
+// Keys per sort tile: one 256-digit histogram per tile, so scratch sized for
+// n keys holds 256 * sort_num_tiles(n) histogram words.
+constexpr uint32_t kSortTileKeys = 4096;
 uint32_t sort_num_tiles(uint32_t n);
 void launch_radix_sort(uint32_t n, uint32_t key_bits, const uint32_t* keys_in, uint32_t* ka, uint32_t* ia,
                        uint32_t* kb, uint32_t* ib, uint32_t* hist, uint32_t* totals, uint32_t** out_keys,
