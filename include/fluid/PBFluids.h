@@ -1,6 +1,6 @@
 // fluid/PBFluids.h — position-based fluids solver, B200 engine.
 //
-// Drop-in for the reference's include/fluid/PBFluids.h:191-371: the same public
+// Drop-in for the reference's include/fluid/PBFluids.h:88-163: the same public
 // members with the same meaning, backed by the C ABI of pbf_b200.h (one CUDA
 // stream and one set of device buffers per instance).  Empty or unready states
 // stay silent no-ops as in the reference; device errors are reported on stderr

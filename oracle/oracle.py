@@ -58,6 +58,50 @@ class DerivedParams(C.Structure):
     ]
 
 
+def derive_f32(cfg, pad=0.0):
+    """PBFluids::setParams in float32 arithmetic (src/fluid/PBFluids.cpp:39-109):
+    the FluidConfigUBO the reference uploads for a FluidConfig-shaped `cfg`.
+    `pad` is the collision padding that setBounds moves the walls in by (:299-306)."""
+    d = DerivedParams()
+    h = np.float32(cfg.h)
+    PI = np.float32(3.14159265358979323846)
+    for a in range(3):
+        d.bounds_min[a] = np.float32(cfg.bounds_min[a]) + np.float32(pad)
+        d.bounds_max[a] = np.float32(cfg.bounds_max[a]) - np.float32(pad)
+        d.gravity_dt[a] = cfg.gravity[a]
+    d.gravity_dt[3] = np.float32(cfg.dt) / np.float32(cfg.substep_iterations)
+    dq = np.float32(cfg.delta_q) * h
+    h2 = h * h
+    r2 = dq * dq + np.float32(0) * np.float32(0) + np.float32(0) * np.float32(0)
+    if r2 > h2:
+        d.wq = 0.0
+    else:
+        h4 = h2 * h2
+        h9k = h4 * h4 * h
+        diff = h2 - r2
+        d.wq = (np.float32(315.0) / (np.float32(64.0) * PI)) / h9k * (diff * diff * diff)
+    d.h, d.rho0, d.eps = cfg.h, cfg.rho0, cfg.eps
+    d.k_corr, d.n_corr, d.viscosity = cfg.k_corr, cfg.n_corr, cfg.viscosity
+    d.bound_damping = min(max(np.float32(cfg.bound_damping), np.float32(0)), np.float32(1))
+    d.hash_size, d.particle_count = cfg.hash_size, cfg.particle_count
+    d.enable_scorr, d.enable_viscosity = cfg.enable_scorr, cfg.enable_viscosity
+    d.cohesion_strength = cfg.cohesion_strength
+    d.interaction_radius, d.interaction_strength = cfg.interaction_radius, cfg.interaction_strength
+    h3 = h2 * h
+    h6 = h3 * h3
+    h9 = h6 * h3
+    d.w0_self = (np.float32(315.0) / (np.float32(64.0) * PI)) / h3
+    d.poly6_coeff = np.float32(315.0) / (np.float32(64.0) * PI * h9)
+    d.spiky_coeff = np.float32(45.0) / (PI * h6)
+    d.inv_rho0 = np.float32(1.0) / np.float32(cfg.rho0)
+    d.hash_mask = cfg.hash_size - 1
+    d.min_lod = cfg.min_lod if cfg.enable_apbf else cfg.solver_iterations
+    d.max_lod = cfg.max_lod if cfg.enable_apbf else cfg.solver_iterations
+    d.lod_max_dist = cfg.lod_max_dist
+    d.enable_apbf = cfg.enable_apbf
+    return d
+
+
 class OrcParams(C.Structure):
     _fields_ = [
         ("bmin", C.c_double * 3), ("bmax", C.c_double * 3), ("g", C.c_double * 3), ("dt", C.c_double),
@@ -87,7 +131,7 @@ class ContactCandidate(C.Structure):
 def build():
     """Compile liboracle.so (and the reference builds when the tree exists)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    ref = os.environ.get("PBF_REFERENCE_TREE", "/root/reference")
+    ref = os.environ.get("PBF_REFERENCE_TREE") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
     if os.path.isdir(ref):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref}"], check=True)
 

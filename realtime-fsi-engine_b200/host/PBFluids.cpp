@@ -1,5 +1,5 @@
 // PBFluids.cpp / SDFBoundary — the reference's C++ fluid interface
-// (include/fluid/PBFluids.h:191-371, include/fluid/SDFBoundary.h:38-167)
+// (include/fluid/PBFluids.h:88-163, include/fluid/SDFBoundary.h:38-167)
 // implemented over the C ABI of pbf_b200.h.
 #include "fluid/PBFluids.h"
 
@@ -7,6 +7,7 @@
 #include <cstring>
 
 #include "pbf_b200.h"
+#include "config_c.h"
 
 // ---- SDFBoundary -------------------------------------------------------------------------
 SDFBoundary::SDFBoundary() : SDFBoundary(0) {}
@@ -105,9 +106,9 @@ SDFBoundary::ClosestSurface SDFBoundary::closestTriangle(const PVec3& p) const
 }
 
 // ---- PBFluids ---------------------------------------------------------------------------------
-void PBFluids::toC(const FluidConfig& p, void* out)
+void pbfhost::fluid_config_to_c(const FluidConfig& p, pbf_fluid_config* out)
 {
-    pbf_fluid_config& c = *static_cast<pbf_fluid_config*>(out);
+    pbf_fluid_config& c = *out;
     std::memset(&c, 0, sizeof(c));
     c.dt = p.dt;
     c.gravity[0] = p.gravity.x; c.gravity[1] = p.gravity.y; c.gravity[2] = p.gravity.z;
@@ -143,6 +144,46 @@ void PBFluids::toC(const FluidConfig& p, void* out)
     c.max_lod = p.maxLOD;
     c.lod_max_dist = p.lodMaxDist;
 }
+
+FluidConfig pbfhost::fluid_config_from_c(const pbf_fluid_config& c)
+{
+    FluidConfig p;
+    p.dt = c.dt;
+    p.gravity = {c.gravity[0], c.gravity[1], c.gravity[2]};
+    p.h = c.h;
+    p.rho0 = c.rho0;
+    p.solverIterations = c.solver_iterations;
+    p.substepIterations = c.substep_iterations;
+    p.eps = c.eps;
+    p.particleCount = c.particle_count;
+    p.spawnMin = {c.spawn_min[0], c.spawn_min[1], c.spawn_min[2]};
+    p.spawnMax = {c.spawn_max[0], c.spawn_max[1], c.spawn_max[2]};
+    p.spawnRandom = c.spawn_random != 0;
+    p.spacing = c.spacing;
+    p.initialVelocity = {c.initial_velocity[0], c.initial_velocity[1], c.initial_velocity[2]};
+    p.boundsMin = {c.bounds_min[0], c.bounds_min[1], c.bounds_min[2]};
+    p.boundsMax = {c.bounds_max[0], c.bounds_max[1], c.bounds_max[2]};
+    p.boundDamping = c.bound_damping;
+    p.hashSize = c.hash_size;
+    p.enableSCorr = c.enable_scorr != 0;
+    p.kCorr = c.k_corr;
+    p.nCorr = c.n_corr;
+    p.deltaQ = c.delta_q;
+    p.cohesionStrength = c.cohesion_strength;
+    p.enableViscosity = c.enable_viscosity != 0;
+    p.viscosity = c.viscosity;
+    p.interactionRadius = c.interaction_radius;
+    p.interactionStrength = c.interaction_strength;
+    p.enableVorticity = c.enable_vorticity != 0;
+    p.vorticityEpsilon = c.vorticity_epsilon;
+    p.enableAPBF = c.enable_apbf != 0;
+    p.minLOD = c.min_lod;
+    p.maxLOD = c.max_lod;
+    p.lodMaxDist = c.lod_max_dist;
+    return p;
+}
+
+void PBFluids::toC(const FluidConfig& p, void* out) { pbfhost::fluid_config_to_c(p, static_cast<pbf_fluid_config*>(out)); }
 
 void PBFluids::report(int rc, const char* what) const
 {

@@ -1,7 +1,7 @@
 """pbf_b200 — Python mirror of the reference's fluid-solver interface.
 
 ``PBFluids`` and ``SDFBoundary`` keep the member names, argument meaning and
-silent no-op behaviour of the reference classes (include/fluid/PBFluids.h:191-371,
+silent no-op behaviour of the reference classes (include/fluid/PBFluids.h:88-163,
 include/fluid/SDFBoundary.h:38-167); each call goes through the C ABI of
 include/pbf_b200.h into the sm_100a kernels of ``libpbf_b200.so``.  Outputs that
 the C++ reference returns through ``std::vector&`` out-parameters are returned
@@ -192,7 +192,7 @@ class GridSDF:
 
 
 class PBFluids:
-    """Position-based fluids solver (include/fluid/PBFluids.h:191-371)."""
+    """Position-based fluids solver (include/fluid/PBFluids.h:88-163)."""
 
     def __init__(self, p=None, device=0):
         self._h = C.c_void_p()

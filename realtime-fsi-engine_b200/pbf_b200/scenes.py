@@ -11,15 +11,21 @@ configurations:
   C3  64 independent dam breaks, N_i ~ U[4096, 131072] (seed 7)
   C4  differentiable C0 scene, 16 substeps x 4 iterations, sphere r=0.15
 
-Constants the configurations leave open are fixed here and listed in DESIGN.md
-(cohesion 0.001, damping 0.5, H = smallest power of two >= max(2^17, N), the
-C1 box height, the C2 capsule's y and length, the C4 sphere centre).
+Constants the configurations leave open are fixed here (cohesion 0.001,
+damping 0.5, H = smallest power of two >= max(2^17, N), the C1 box height,
+the C2 capsule's y and length, the C4 sphere centre).
 """
 import math
 
 import numpy as np
 
-from ._capi import FluidConfig
+try:
+    from ._capi import FluidConfig
+except ImportError:
+    # Loaded as a stand-alone file, outside the package (a CPU-only caller
+    # that must not load the engine, such as the benchmark's reference arm):
+    # the caller assigns a ctypes struct with pbf_fluid_config's layout.
+    FluidConfig = None
 
 
 def lattice_density(h, d):
