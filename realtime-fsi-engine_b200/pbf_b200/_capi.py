@@ -97,6 +97,16 @@ class DeformParams(C.Structure):
                 ("control_threshold", C.c_float), ("control_threshold_low", C.c_float)]
 
 
+class ScenePreset(C.Structure):
+    """pbf_scene_preset (include/core/Scene.h:29-67 as a C struct)."""
+
+    _fields_ = [("name", C.c_char * 48), ("fluid", FluidConfig), ("cam_yaw", C.c_float), ("cam_pitch", C.c_float),
+                ("cam_dist", C.c_float), ("point_size", C.c_float), ("mesh_file", C.c_char * 64),
+                ("mesh_fit_size", C.c_float), ("sdf_cell", C.c_float), ("sdf_padding", C.c_float),
+                ("sdf_container", C.c_uint32), ("mesh_translate", C.c_float * 3), ("mesh_rot_deg", C.c_float * 3),
+                ("deform", DeformParams), ("local_kring", C.c_int32), ("contact_radius", C.c_float)]
+
+
 BATCH_ALL = 0xFFFFFFFF
 BOPT_BLOCK, BOPT_ORDER, BOPT_BLOCKS_PER_SM, BOPT_USE_GRAPH, BOPT_NEIGHBOUR_MODE = 1, 2, 3, 4, 5
 
@@ -193,6 +203,14 @@ SIGNATURES = [
     ("pbf_deform_step", C.c_int, [vp, vp, i32, C.c_float, P(DeformParams), P(i32), P(i32), P(i32)]),
     ("pbf_deform_patch_size", C.c_int, [vp, P(i32)]),
     ("pbf_deform_verify_incremental", C.c_int, [vp, P(C.c_double)]),
+    # scene presets and headless set-up
+    ("pbf_scene_count", C.c_int, []),
+    ("pbf_scene_get", C.c_int, [i32, P(ScenePreset)]),
+    ("pbf_off_load", C.c_int, [C.c_char_p, vp, i32, vp, i32, P(i32), P(i32)]),
+    ("pbf_mesh_fit", C.c_int, [vp, i32, P(C.c_float), C.c_double]),
+    ("pbf_mesh_fit_center", C.c_int, [P(FluidConfig), P(C.c_float)]),
+    ("pbf_mesh_place", C.c_int, [vp, i32, P(C.c_float), P(C.c_float)]),
+    ("pbf_spawn_particles", C.c_int, [P(FluidConfig), vp, u32, P(u32)]),
     # differentiable step
     ("pbf_batch_set_sdf_offset", C.c_int, [vp, u32, P(C.c_float)]),
     ("pbf_batch_set_state", C.c_int, [vp, vp, vp]),
