@@ -24,6 +24,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, os.path.join(ROOT, "realtime-fsi-engine_b200"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 import oracle as O  # noqa: E402
 from pbf_b200 import scenes  # noqa: E402
@@ -31,46 +32,7 @@ from pbf_b200 import scenes  # noqa: E402
 F32 = np.float32
 
 
-def derive_f32(cfg, pad=0.0):
-    """PBFluids::setParams in float32 arithmetic (PBFluids.cpp:39-109)."""
-    d = O.DerivedParams()
-    h = F32(cfg.h)
-    PI = F32(3.14159265358979323846)
-    for a in range(3):
-        d.bounds_min[a] = F32(cfg.bounds_min[a]) + F32(pad)
-        d.bounds_max[a] = F32(cfg.bounds_max[a]) - F32(pad)
-        d.gravity_dt[a] = cfg.gravity[a]
-    d.gravity_dt[3] = F32(cfg.dt) / F32(cfg.substep_iterations)
-    dq = F32(cfg.delta_q) * h
-    h2 = h * h
-    r2 = dq * dq + F32(0) * F32(0) + F32(0) * F32(0)
-    if r2 > h2:
-        d.wq = 0.0
-    else:
-        h4 = h2 * h2
-        h9k = h4 * h4 * h
-        diff = h2 - r2
-        d.wq = (F32(315.0) / (F32(64.0) * PI)) / h9k * (diff * diff * diff)
-    d.h, d.rho0, d.eps = cfg.h, cfg.rho0, cfg.eps
-    d.k_corr, d.n_corr, d.viscosity = cfg.k_corr, cfg.n_corr, cfg.viscosity
-    d.bound_damping = min(max(F32(cfg.bound_damping), F32(0)), F32(1))
-    d.hash_size, d.particle_count = cfg.hash_size, cfg.particle_count
-    d.enable_scorr, d.enable_viscosity = cfg.enable_scorr, cfg.enable_viscosity
-    d.cohesion_strength = cfg.cohesion_strength
-    d.interaction_radius, d.interaction_strength = cfg.interaction_radius, cfg.interaction_strength
-    h3 = h2 * h
-    h6 = h3 * h3
-    h9 = h6 * h3
-    d.w0_self = (F32(315.0) / (F32(64.0) * PI)) / h3
-    d.poly6_coeff = F32(315.0) / (F32(64.0) * PI * h9)
-    d.spiky_coeff = F32(45.0) / (PI * h6)
-    d.inv_rho0 = F32(1.0) / F32(cfg.rho0)
-    d.hash_mask = cfg.hash_size - 1
-    d.min_lod = cfg.min_lod if cfg.enable_apbf else cfg.solver_iterations
-    d.max_lod = cfg.max_lod if cfg.enable_apbf else cfg.solver_iterations
-    d.lod_max_dist = cfg.lod_max_dist
-    d.enable_apbf = cfg.enable_apbf
-    return d
+derive_f32 = O.derive_f32
 
 
 def to_oracle_cfg(cfg):
@@ -184,6 +146,38 @@ def run_glsl(cfg, pos, vel, sdf=None, sort_mode=0, interaction=None, camera=(0, 
     return rec
 
 
+def gen_c0_scorr(out):
+    """Config-0 first substep with s_corr: for each ensemble member the
+    reference shaders' x* after every solver iteration and the committed
+    positions, compared with FP64 on the same inputs (statistics only), plus
+    member 0's committed FP32 positions for a direct GPU-vs-reference
+    distance."""
+    import c0_scorr as Z
+    cfg, pos, vel = Z.scene()
+    n, h = len(pos), float(cfg.h)
+    iters = cfg.solver_iterations
+    ref_stats = np.zeros((Z.N_MEMBERS, iters + 1, len(Z.STAT_NAMES)))
+    ref_pos0 = None
+    for m in range(Z.N_MEMBERS):
+        pp = Z.member_inputs(pos, m)
+        f64 = Z.fp64_stages(cfg, pp, vel)
+        S = O.GlslScene(derive_f32(cfg), to_oracle_cfg(cfg), pp, vel, parallel=True)
+        for st in (1, 2, 3):
+            S.stage(st)
+        for it in range(1, iters + 1):
+            S.stage(5, it)
+            S.stage(6, it)
+            S.stage(7, it)
+            ref_stats[m, it - 1] = Z.stats(S.solver[:, 0:3], f64[f"xstar{it}"], h)
+        S.stage(8)
+        ref_stats[m, iters] = Z.stats(S.pos, f64["pos"], h)
+        if m == 0:
+            ref_pos0 = S.pos.astype(np.float32).copy()
+    np.savez_compressed(out, ref_stats=ref_stats, ref_pos0=ref_pos0,
+                        pos0_sum=np.array([pos.astype(np.float64).sum(), (pos.astype(np.float64) ** 2).sum()]),
+                        n=np.int64(n))
+
+
 def save_scene(out, cfg, pos, vel, rec, sdf=None, extra=None):
     payload = dict(pos0=pos, vel0=vel, **{"cfg_" + k: v for k, v in cfg_dict(cfg).items()}, **rec)
     if sdf is not None:
@@ -238,6 +232,8 @@ def main():
     cnt = int(S.count[0])
     save_scene(os.path.join(HERE, "glsl_contacts.npz"), cfg, pos, vel,
                dict(contacts=S.contacts[:cnt].copy(), band=np.float32(0.03)), sdf=sdf)
+    # 8) config-0 first substep with s_corr, ensemble statistics
+    gen_c0_scorr(os.path.join(HERE, "glsl_c0_scorr.npz"))
     print("golden fixtures written to", HERE)
 
 
