@@ -50,8 +50,13 @@ def parse():
                          "c3: 64-scene batch vs the same scenes stepped one by one; "
                          "c4: differentiable step (adjoint cost and gradient checks)")
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0,
+                    help="host seconds of the 64^3 sub-block CPU baseline")
+    ap.add_argument("--ref-seconds", type=float, default=30.0,
+                    help="host seconds of the reference arm's timed steps on the full scene")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="c2 only: skip the short C3 batch and C4 adjoint runs attached to the line")
     ap.add_argument("--mode", type=int, default=-1, choices=[-1, 0, 1, 2, 3, 4, 5, 6, 7, 8],
                     help="neighbour passes: -1 automatic (default: 8 from 2^19 particles, else 4), 0 hash order, "
                          "1 Morton, 2 Morton cell-cooperative, 3 Morton with per-lane pair queues, 4 Morton with "
@@ -145,17 +150,23 @@ class Clocks:
 
 
 # ---- scenes ------------------------------------------------------------------------------
+def workload_desc(name):
+    if name == "c0":
+        return "dam break 32^3 (32,768 particles, d=0.02, h=0.04, S=2, I=4)"
+    return ("dam break 256x128x128 (4,194,304 particles, d=0.005, h=0.01, S=1 at dt=1/120, I=4, "
+            "capsule SDF r=0.1 at x=1.2)")
+
+
 def workload(name, sample=None):
     from pbf_b200 import scenes
     if name == "c0":
         cfg, pos, vel = scenes.c0(32)
-        return cfg, pos, vel, None, "dam break 32^3 (32,768 particles, d=0.02, h=0.04, S=2, I=4)"
+        return cfg, pos, vel, None, workload_desc("c0")
     if sample:
         cfg, pos, vel, sdf = scenes.c2(nx=sample[0], ny=sample[1], nz=sample[2])
     else:
         cfg, pos, vel, sdf = scenes.c2()
-    return cfg, pos, vel, sdf, ("dam break 256x128x128 (4,194,304 particles, d=0.005, h=0.01, S=1 at dt=1/120, I=4, "
-                                "capsule SDF r=0.1 at x=1.2)")
+    return cfg, pos, vel, sdf, workload_desc("c2")
 
 
 def peaks():
@@ -176,59 +187,93 @@ def traffic_summary(mode):
 
 
 # ---- CPU reference / baseline -------------------------------------------------------------------
-def cpu_reference_rate(budget_s):
-    """The reference's own compute shaders, compiled as C++ and run with
-    OpenMP on the host cores (oracle/_ref), on a 64^3 sub-block of the same
-    workload; falls back to the FP64 oracle port when _ref is absent."""
+def reference_side():
+    """The oracle module and the scene generators, loaded without the engine
+    package (the reference arm must not load or run any of the engine)."""
+    import importlib.util
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    cfg, pos, vel, sdf, _ = workload("c2", sample=(64, 64, 64))
+    path = os.path.join(ROOT, "realtime-fsi-engine_b200", "pbf_b200", "scenes.py")
+    spec = importlib.util.spec_from_file_location("pbf_scenes_standalone", path)
+    S = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(S)
+    S.FluidConfig = O.FluidConfig  # same layout as pbf_fluid_config
+    return O, S
+
+
+def cpu_reference_rate(budget_s, sample=(64, 64, 64), max_steps=50, warmup=0):
+    """The reference's own compute shaders, compiled as C++ and run with
+    OpenMP on the host cores (oracle/_ref), with the UBO derived by the
+    reference's setParams float arithmetic (oracle.derive_f32), on the C2
+    workload (`sample` = None) or a sub-block of its lattice; falls back to the
+    FP64 oracle port when _ref is absent.  Steps run until `budget_s` seconds
+    or `max_steps` steps, at least one."""
+    O, S = reference_side()
+    if sample:
+        cfg, pos, vel, sdf = S.c2(nx=sample[0], ny=sample[1], nz=sample[2])
+    else:
+        cfg, pos, vel, sdf = S.c2()
     n = len(pos)
     grid, origin, cell, pad = sdf
     osdf = O.Sdf(grid, origin, cell, padding=pad, containment=False)
-    ocfg = O.FluidConfig()
-    C.memmove(C.byref(ocfg), C.byref(cfg), C.sizeof(ocfg))
     cores = os.cpu_count() or 1
-    sample = f"64x64x64 sub-block of the 4M lattice ({n} particles, same d/h/constants/capsule)"
-    steps = 0
-    t0 = time.perf_counter()
+    what = (f"{sample[0]}x{sample[1]}x{sample[2]} sub-block of the 4M lattice ({n} particles, same d/h/constants/"
+            "capsule)" if sample else f"the full C2 scene ({n} particles)")
     if O.have_ref():
-        import pbf_b200 as P
-        d = O.DerivedParams()
-        C.memmove(C.byref(d), C.byref(P.derive_params(cfg)), C.sizeof(d))
-        S = O.GlslScene(d, ocfg, pos, vel, sdf=osdf, sort_mode=0, parallel=True, pre_integrate=True)
         kind = "reference"
-        while True:
-            S.step()
-            steps += 1
-            if time.perf_counter() - t0 > budget_s or steps >= 50:
-                break
+        scene = O.GlslScene(O.derive_f32(cfg), cfg, pos, vel, sdf=osdf, sort_mode=0, parallel=True,
+                            pre_integrate=True)
+        one = scene.step
     else:
         kind = "port"
-        p = O.Params(ocfg)
+        p = O.Params(cfg)
         p64, v64 = pos.astype(np.float64), vel.astype(np.float64)
-        while True:
+
+        def one():
             O.step(p, p64, v64, sdf=osdf)
-            steps += 1
-            if time.perf_counter() - t0 > budget_s or steps >= 50:
-                break
+    for _ in range(warmup):
+        one()
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        one()
+        steps += 1
+        if time.perf_counter() - t0 > budget_s or steps >= max_steps:
+            break
     dt = time.perf_counter() - t0
     rate = n * cfg.substep_iterations * steps / dt
     return {"value": rate, "unit": METRIC, "cores": cores, "kind": kind,
-            "sample": f"{sample}, {steps} steps in {dt:.1f} s, OpenMP over {cores} host threads"}
+            "sample": f"{what}, {steps} steps in {dt:.1f} s after {warmup} warm-up, OpenMP over {cores} "
+                      "host threads"}, cfg
 
 
-def run_reference(args, dist):
-    if dist.rank != 0:
+def c2_config(desc, cfg, n):
+    """The workload's config object, identical in both arms."""
+    return {"workload": desc, "particles_per_gpu": n, "substeps": int(cfg.substep_iterations),
+            "solver_iterations": int(cfg.solver_iterations), "hash_size": int(cfg.hash_size),
+            "l2": "working set >> 126 MB L2 (no flush needed)"}
+
+
+def run_reference(args):
+    """The reference arm: the reference's shaders on the host cores, on the
+    full 4,194,304-particle scene (one warm-up step, then steps until
+    --ref-seconds; a few minutes at most).  Under torchrun only rank 0 runs."""
+    if int(os.environ.get("RANK", "0")) != 0:
         return
-    cb = cpu_reference_rate(args.cpu_seconds)
-    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": METRIC, "n_gpus": args.gpus,
+    if args.workload != "c2":
+        print(json.dumps({"impl": "reference", "unavailable": f"the reference arm times the c2 workload only, "
+                                                              f"not {args.workload}"}), flush=True)
+        return
+    full, cfg = cpu_reference_rate(args.ref_seconds, sample=None, max_steps=max(1, args.steps),
+                                   warmup=min(args.warmup, 1))
+    desc = workload_desc("c2")
+    n = int(cfg.particle_count)
+    line = {"impl": "reference", "metric": METRIC, "value": full["value"], "unit": METRIC, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": workload(args.workload)[4] if args.workload == "c0" else
-                       "dam break 4,194,304 particles (timed on a 64^3 sub-block on the host)"},
-            "cpu_baseline": cb,
-            "e2e": {"value": cb["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "config": c2_config(desc, cfg, n), "parallelism": f"{full['cores']} host threads",
+            "cpu_baseline": full,
+            "e2e": {"value": full["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -344,26 +389,52 @@ def run_b200(args, dist):
                 "note": "neighbour passes are FP32-issue / L1 bound; algorithmic bytes = inputs + outputs once"}
     cb = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
-        cb = cpu_reference_rate(args.cpu_seconds)
+        cb, _ = cpu_reference_rate(args.cpu_seconds)
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": dist.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": desc, "particles_per_gpu": n, "substeps": subs,
-                       "solver_iterations": cfg.solver_iterations, "hash_size": cfg.hash_size,
-                       "neighbour_mode": mode,
-                       "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU",
-                       "l2": "working set >> 126 MB L2 (no flush needed)"},
+            "config": c2_config(desc, cfg, n), "neighbour_mode": mode,
+            "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU",
             "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
             "passes": per_pass, "nonfinite_particles": int(bad), "impl": "b200"}
     if ws1 is not None:
         # pbf_list_stats before and after the timed steps (meaning per mode in pbf_b200.h)
         line["walk_stats"] = {"before": list(ws0), "after": list(ws1)}
+    del fl, obstacle
+    if args.workload == "c2" and not args.no_extras and not args.sample:
+        line.update(extra_workloads(args, dist))
     if dist.rank == 0:
         print(json.dumps(line), flush=True)
-    del obstacle
 
 
-def run_batch(args, dist):
+def extra_workloads(args, dist):
+    """Short runs of the two other figures the headline metric names, attached
+    to the C2 line: the 64-scene batch against the same scenes stepped one by
+    one (C3), and the adjoint/forward time ratio at 16 scenes with the
+    smooth-variant gradient check against FP64 central differences (C4)."""
+    import copy
+    sub = copy.copy(args)
+    sub.steps, sub.warmup, sub.e2e_steps = 5, 3, 2
+    c3 = run_batch(sub, dist, emit=False)
+    out = {"c3": {"value": c3["value"], "unit": METRIC, "ms_per_step": c3["ms_per_step"],
+                  "sequential_ms_per_step": c3["sequential"]["ms_per_step"],
+                  "speedup_vs_sequential": c3["speedup_vs_sequential"],
+                  "max_pos_diff_vs_sequential": c3["max_pos_diff_vs_sequential"],
+                  "particles": c3["config"]["particles_total"], "autotune_best": c3["autotune"]["best"],
+                  "steps": sub.steps, "warmup": sub.warmup, "clocks": c3["clocks"],
+                  "workload": c3["config"]["workload"]}}
+    c4 = run_adjoint(sub, dist, emit=False, variants=("smooth",))
+    gc = (c4.get("gradcheck") or {}).get("smooth (s_corr off, cohesion 0)") or {}
+    out["c4"] = {"adjoint_over_forward_16_scenes": c4["value"], "costs": c4["costs"],
+                 "gradcheck_smooth": {k: gc.get(k) for k in ("max_rel_gpu_vs_fd64", "max_rel_fp64_adjoint_vs_fd64",
+                                                              "rel_vs_fp64_cpu_adjoint_velocity",
+                                                              "rel_vs_fp64_cpu_adjoint_translation", "fd_eps")},
+                 "steps": sub.steps, "warmup": sub.warmup, "clocks": c4["clocks"],
+                 "workload": c4["config"]["workload"]}
+    return out
+
+
+def run_batch(args, dist, emit=True):
     """C3: 64 independent dam breaks in one multi-scene batch (one launch per
     pass, CUDA graph, autotuned launch shape), against the same scenes stepped
     one by one with one single-scene handle each.  With N ranks the scenes are
@@ -468,12 +539,13 @@ def run_batch(args, dist):
             "e2e": {"value": n_all * subs * args.e2e_steps / e2e_s, "unit": METRIC, "h2d_bytes_per_step": n * 48,
                     "d2h_bytes_per_step": n * 48},
             "roofline": None, "cpu_baseline": None, "gpu_launches": int(launches), "clocks": clk, "impl": "b200"}
-    if dist.rank == 0:
+    if emit and dist.rank == 0:
         print(json.dumps(line), flush=True)
-    del seq, seq_by_mode
+    del seq, seq_by_mode, b
+    return line
 
 
-def run_adjoint(args, dist):
+def run_adjoint(args, dist, emit=True, variants=("smooth", "cohesion", "configured")):
     """C4: differentiable C0 scene (32,768 particles, 16 substeps x 4
     iterations in one step, sphere obstacle r=0.15).  Times the forward step,
     the recording forward and the backward on 1 scene and on 16 scenes in
@@ -606,14 +678,16 @@ def run_adjoint(args, dist):
                            max_rel_fp64_adjoint_vs_fd64=max(d["rel_fp64_adjoint"] for d in dirs))
             return out
 
-        checks = {
-            "smooth (s_corr off, cohesion 0)": against_fp64(variant(0, 0.0), 8),
-            "s_corr off, cohesion 0.001": against_fp64(variant(0, 0.001), 0),
-            "as configured (s_corr k=0.1, cohesion 0.001)": against_fp64(cfg, 0),
-            "note": ("cohesion 0.001 puts the max(C, -cohesion) kink inside the jittered lattice's density "
-                     "fluctuations, where FP32 and FP64 take different branches; with s_corr k=0.1 at unit "
-                     "mass the step's tangent map has a norm ~1e43 and no gradient is usable in any precision"),
-        }
+        checks = {}
+        if "smooth" in variants:
+            checks["smooth (s_corr off, cohesion 0)"] = against_fp64(variant(0, 0.0), 8)
+        if "cohesion" in variants:
+            checks["s_corr off, cohesion 0.001"] = against_fp64(variant(0, 0.001), 0)
+        if "configured" in variants:
+            checks["as configured (s_corr k=0.1, cohesion 0.001)"] = against_fp64(cfg, 0)
+        checks["note"] = ("cohesion 0.001 puts the max(C, -cohesion) kink inside the jittered lattice's density "
+                          "fluctuations, where FP32 and FP64 take different branches; with s_corr k=0.1 at unit "
+                          "mass the step's tangent map has a norm ~1e43 and no gradient is usable in any precision")
     line = {"metric": "adjoint/forward time ratio (16 scenes)", "value": ratio, "unit": "x", "n_gpus": dist.world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": costs[16]["backward_ms"],
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -622,8 +696,9 @@ def run_adjoint(args, dist):
                        "l2": "16-scene working set > 126 MB L2"},
             "costs": costs, "gradcheck": checks, "clocks": clk, "roofline": None, "cpu_baseline": None,
             "impl": "b200"}
-    if dist.rank == 0:
+    if emit and dist.rank == 0:
         print(json.dumps(line), flush=True)
+    return line
 
 
 def run_coupled(args, dist):
@@ -687,11 +762,12 @@ def run_coupled(args, dist):
 
 def main():
     args = parse()
+    if args.impl == "reference":
+        run_reference(args)  # host only: no process group, no GPU
+        return
     dist = Dist(args.gpus)
     try:
-        if args.impl == "reference":
-            run_reference(args, dist)
-        elif args.workload == "c1":
+        if args.workload == "c1":
             run_coupled(args, dist)
         elif args.workload == "c3":
             run_batch(args, dist)
