@@ -6,6 +6,7 @@ CPU-baseline legs of bench.py, never by the product path.
   liboracle.so         FP64 restatement (oracle/pbf_oracle.c, sdf_oracle.c)
   _ref/libpbfref_cpu.so   reference src/fluid/Kernels.cpp + NeighborSearch.cpp
   _ref/libpbfref_glsl.so  reference compute shaders run on the CPU
+  _ref/libpbfref_sdf.so   reference src/fluid/SDFBoundary.cpp (mesh SDF, BVH)
 """
 import ctypes as C
 import os
@@ -18,6 +19,7 @@ ROOT = os.path.dirname(HERE)
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 REF_CPU_PATH = os.path.join(HERE, "_ref", "libpbfref_cpu.so")
 REF_GLSL_PATH = os.path.join(HERE, "_ref", "libpbfref_glsl.so")
+REF_SDF_PATH = os.path.join(HERE, "_ref", "libpbfref_sdf.so")
 
 f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
@@ -338,6 +340,74 @@ def ref_glsl():
         L.glsl_ref_step.argtypes = [C.POINTER(GlslCtx)]
         _ref_glsl = L
     return _ref_glsl
+
+
+_ref_sdf = None
+
+
+def ref_sdf():
+    global _ref_sdf
+    if _ref_sdf is None:
+        L = C.CDLL(REF_SDF_PATH)
+        L.sdfref_build.argtypes = [f64p, C.c_int, i32p, C.c_int, C.c_double]
+        L.sdfref_build.restype = C.c_void_p
+        L.sdfref_free.argtypes = [C.c_void_p]
+        L.sdfref_grid_info.argtypes = [C.c_void_p, i32p, f64p, C.POINTER(C.c_double)]
+        L.sdfref_grid.argtypes = [C.c_void_p, f32p]
+        L.sdfref_refit.argtypes = [C.c_void_p, f64p, C.c_int]
+        L.sdfref_refit_dirty.argtypes = [C.c_void_p, f64p, C.c_int, C.c_double, C.c_double]
+        L.sdfref_refit_dirty.restype = C.c_int
+        L.sdfref_closest.argtypes = [C.c_void_p, f32p, C.c_int, i32p, f32p]
+        _ref_sdf = L
+    return _ref_sdf
+
+
+def have_ref_sdf():
+    return os.path.exists(REF_SDF_PATH)
+
+
+class RefSDF:
+    """The reference's own SDFBoundary (buildFromMesh / refitFromMesh /
+    refitDirty / closestTriangle) over a triangle mesh."""
+
+    def __init__(self, verts, faces, cell):
+        V = np.ascontiguousarray(verts, np.float64).reshape(-1, 3)
+        F = np.ascontiguousarray(faces, np.int32).reshape(-1, 3)
+        self.nv = len(V)
+        self.h = ref_sdf().sdfref_build(V.reshape(-1), len(V), F.reshape(-1), len(F), float(cell))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            ref_sdf().sdfref_free(self.h)
+            self.h = None
+
+    def info(self):
+        dims = np.zeros(3, np.int32)
+        org = np.zeros(3)
+        c = C.c_double()
+        ref_sdf().sdfref_grid_info(self.h, dims, org, C.byref(c))
+        return dims, org, c.value
+
+    def grid(self):
+        dims = self.info()[0]
+        out = np.zeros(int(np.prod(dims)), np.float32)
+        ref_sdf().sdfref_grid(self.h, out)
+        return out
+
+    def refit(self, verts):
+        V = np.ascontiguousarray(verts, np.float64).reshape(-1)
+        ref_sdf().sdfref_refit(self.h, V, self.nv)
+
+    def refit_dirty(self, verts, band, move_eps):
+        V = np.ascontiguousarray(verts, np.float64).reshape(-1)
+        return bool(ref_sdf().sdfref_refit_dirty(self.h, V, self.nv, float(band), float(move_eps)))
+
+    def closest(self, pts):
+        P = np.ascontiguousarray(pts, np.float32).reshape(-1, 3)
+        face = np.zeros(len(P), np.int32)
+        pt = np.zeros((len(P), 3), np.float32)
+        ref_sdf().sdfref_closest(self.h, P.reshape(-1), len(P), face, pt.reshape(-1))
+        return face, pt
 
 
 def have_ref():

@@ -178,6 +178,32 @@ def gen_c0_scorr(out):
                         n=np.int64(n))
 
 
+def gen_sdf_ref(out):
+    """The reference's own SDFBoundary (src/fluid/SDFBoundary.cpp, compiled by
+    oracle/Makefile) on an icosphere: the grid after buildFromMesh, after
+    refitFromMesh of seeded moved vertices (build-time edge and vertex
+    pseudo-normals kept), after buildFromMesh of the moved vertices (all
+    pseudo-normals recomputed), and closestTriangle points at seeded
+    queries."""
+    V, F = scenes.icosphere(2, 0.2, (0.8, 0.3, 0.5))
+    cell = 0.025
+    rng = np.random.default_rng(21)
+    V2 = V + rng.normal(0.0, 0.01, V.shape)
+    V2[:20] += [0.0, 0.06, 0.0]  # a dent well beyond the noise
+    R = O.RefSDF(V, F, cell)
+    dims, org, c = R.info()
+    grid = R.grid()
+    pts = (rng.uniform(-0.3, 0.3, (500, 3)) + [0.8, 0.3, 0.5]).astype(np.float32)
+    face, point = R.closest(pts)
+    R.refit(V2)
+    refit = R.grid()
+    R2 = O.RefSDF(V2, F, cell)
+    dims2, org2, _ = R2.info()
+    np.savez_compressed(out, verts=V, faces=F.astype(np.int32), verts_moved=V2, cell=np.float64(cell), dims=dims,
+                        origin=org, grid=grid, refit_grid=refit, rebuild_dims=dims2, rebuild_origin=org2,
+                        rebuild_grid=R2.grid(), query=pts, closest_face=face, closest_point=point)
+
+
 def save_scene(out, cfg, pos, vel, rec, sdf=None, extra=None):
     payload = dict(pos0=pos, vel0=vel, **{"cfg_" + k: v for k, v in cfg_dict(cfg).items()}, **rec)
     if sdf is not None:
@@ -232,7 +258,9 @@ def main():
     cnt = int(S.count[0])
     save_scene(os.path.join(HERE, "glsl_contacts.npz"), cfg, pos, vel,
                dict(contacts=S.contacts[:cnt].copy(), band=np.float32(0.03)), sdf=sdf)
-    # 8) config-0 first substep with s_corr, ensemble statistics
+    # 8) the reference's mesh SDF: build, refit, rebuild, closest points
+    gen_sdf_ref(os.path.join(HERE, "sdf_ref.npz"))
+    # 9) config-0 first substep with s_corr, ensemble statistics
     gen_c0_scorr(os.path.join(HERE, "glsl_c0_scorr.npz"))
     print("golden fixtures written to", HERE)
 

@@ -188,3 +188,89 @@ def test_deform_step_handle_policy(sphere):
         assert moved == bool(handles or refactored)
         assert np.abs(d.vertices() - cur).max() < 1e-8, frame
         last = handles
+
+
+def _script(n, A, rng, steps=8):
+    """Constraint masks (a growing and shrinking contact patch), full or
+    column-update factorizations with the changed columns (entering/leaving
+    vertices and their neighbours), random right-hand sides."""
+    import scipy.sparse as sp
+    Ac = sp.csc_matrix(A)
+    Ac.sort_indices()
+    masks = np.zeros((steps, n), np.int8)
+    full = np.zeros(steps, np.int32)
+    changed, cptr = [], [0]
+    prev = np.zeros(n, bool)
+    for s in range(steps):
+        cur = prev.copy()
+        if s == 0:
+            cur[rng.choice(n, 12, replace=False)] = True
+            full[s] = 1
+        else:
+            cur[rng.choice(n, 5, replace=False)] = True
+            cur[rng.choice(np.flatnonzero(cur), 3, replace=False)] = False
+            full[s] = 1 if s == steps - 1 else 0
+        diff = np.flatnonzero(cur != prev)
+        ch = set(diff.tolist())
+        for k in diff:
+            ch.update(Ac.indices[Ac.indptr[k]:Ac.indptr[k + 1]].tolist())
+        changed += sorted(ch)
+        cptr.append(len(changed))
+        masks[s] = cur
+        prev = cur
+    rhs = rng.normal(size=(steps, n))
+    return (Ac.indptr.astype(np.int32), Ac.indices.astype(np.int32), Ac.data.astype(np.float64), masks, full,
+            np.array(cptr, np.int32), np.array(changed, np.int32), rhs)
+
+
+def _run(fn, n, script):
+    import ctypes as C
+    p, i, x, masks, full, cptr, ch, rhs = script
+    out = np.zeros_like(rhs)
+    ptr = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    rc = fn(n, ptr(p), ptr(i), ptr(x), len(full), ptr(masks), ptr(full), ptr(cptr), ptr(ch), ptr(rhs), ptr(out))
+    assert rc == 0
+    return out
+
+
+def test_incremental_cholesky_matches_reference_build(tmp_path, sphere):
+    """The library's IncrementalCholesky against the reference's own
+    src/deformation/IncrementalCholesky.cpp (oracle/_ref/libpbfref_chol.so),
+    replaying the same analyze / setConstrained / factorizeFull / updateColumns
+    / solveInPlace script on the C1-style normal matrix of a cotangent
+    Laplacian (2-ring pattern).  Both follow the up-looking LDL^T recurrence
+    in the same order, so the solutions are bit-identical."""
+    import ctypes as C
+    import os
+    import subprocess
+    import oracle as O
+    ref_so = os.path.join(os.path.dirname(O.__file__), "_ref", "libpbfref_chol.so")
+    if not os.path.exists(ref_so):
+        pytest.skip("oracle/_ref not built (needs the reference tree)")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    so = str(tmp_path / "libchol_harness.so")
+    subprocess.run(["/usr/bin/g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-I" + os.path.join(root, "include"),
+                    os.path.join(root, "tests", "cpp", "chol_harness.cpp"),
+                    os.path.join(root, "realtime-fsi-engine_b200", "host", "IncrementalCholesky.cpp"), "-o", so],
+                   check=True, capture_output=True, text=True)
+    mine = C.CDLL(so).chol_run
+    ref = C.CDLL(ref_so).cholref_run
+    for fn in (mine, ref):
+        fn.restype = C.c_int
+    V, F = sphere
+    L, _ = cot_laplacian(V, F)
+    n = len(V)
+    A = L.T @ L + 1e-3 * np.eye(n)
+    A[np.abs(A) < 1e-15] = 0.0
+    script = _script(n, A, np.random.default_rng(4))
+    got, want = _run(mine, n, script), _run(ref, n, script)
+    assert np.array_equal(got, want)
+    # and both solve A^B x = b
+    masks, rhs = script[3], script[7]
+    for s in range(len(rhs)):
+        B = masks[s].astype(bool)
+        AB = A.copy()
+        AB[B, :] = 0.0
+        AB[:, B] = 0.0
+        AB[B, B] = 1.0
+        assert np.abs(AB @ want[s] - rhs[s]).max() < 1e-8 * np.abs(rhs[s]).max()

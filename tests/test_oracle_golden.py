@@ -190,3 +190,76 @@ def test_contact_filter_matches_reference():
     ref = np.sort(z["contacts"][:, :3].copy().view([("", np.float32)] * 3).ravel(), axis=0)
     assert c == len(z["contacts"]) and c > 0
     assert np.array_equal(mine, ref)
+
+
+def _orc_mesh(V, F, cell):
+    V = np.ascontiguousarray(V, np.float64)
+    F = np.ascontiguousarray(F, np.int32)
+    m = O.lib().orc_mesh_build(V.reshape(-1), len(V), F.reshape(-1), len(F), float(cell))
+    dims = np.zeros(3, np.int32)
+    org = np.zeros(3)
+    c = C.c_double()
+    O.lib().orc_mesh_grid_info(m, dims, org, C.byref(c))
+    return m, dims, org
+
+
+def _orc_grid(m, dims):
+    out = np.zeros(int(np.prod(dims)), np.float32)
+    O.lib().orc_mesh_grid(m, out)
+    return out
+
+
+def test_mesh_sdf_matches_reference_sdfboundary():
+    """The mesh half of the oracle (oracle/sdf_oracle.c) against the
+    reference's own SDFBoundary.cpp (fixture sdf_ref.npz): the grid after a
+    build, after a refit of moved vertices (build-time edge and vertex
+    pseudo-normals kept) and after a build of the moved vertices, bit for bit;
+    closest points to float32 rounding (faces may differ only where two faces
+    share the closest point)."""
+    z = H.load("sdf_ref.npz")
+    cell = float(z["cell"])
+    m, dims, org = _orc_mesh(z["verts"], z["faces"], cell)
+    try:
+        assert np.array_equal(dims, z["dims"]) and np.array_equal(org, z["origin"])
+        assert np.array_equal(_orc_grid(m, dims), z["grid"])
+        q = z["query"]
+        pts = np.zeros((len(q), 3))
+        for i, p in enumerate(q):
+            d = C.c_double()
+            pp = np.zeros(3)
+            O.lib().orc_mesh_closest(m, np.ascontiguousarray(p, np.float64), pp, C.byref(d))
+            pts[i] = pp
+        assert np.abs(pts - z["closest_point"]).max() < 1e-7
+        O.lib().orc_mesh_refit(m, np.ascontiguousarray(z["verts_moved"], np.float64).reshape(-1))
+        assert np.array_equal(_orc_grid(m, dims), z["refit_grid"])
+    finally:
+        O.lib().orc_mesh_free(m)
+    m, dims, org = _orc_mesh(z["verts_moved"], z["faces"], cell)
+    try:
+        assert np.array_equal(dims, z["rebuild_dims"]) and np.array_equal(org, z["rebuild_origin"])
+        assert np.array_equal(_orc_grid(m, dims), z["rebuild_grid"])
+    finally:
+        O.lib().orc_mesh_free(m)
+    # a refit and a rebuild of the same moved mesh differ (the stale pseudo-normals)
+    assert not np.array_equal(z["refit_grid"], z["rebuild_grid"][:len(z["refit_grid"])])
+
+
+@pytest.mark.skipif(not O.have_ref_sdf(), reason="oracle/_ref not built (needs the reference tree)")
+@pytest.mark.parametrize("subdiv,cell", [(1, 0.05), (3, 0.02), (4, 0.0125)])
+def test_mesh_sdf_matches_reference_build_on_icospheres(subdiv, cell):
+    """The same comparison on the sphere sizes the GPU tests use, against the
+    reference's SDFBoundary run here (oracle/_ref/libpbfref_sdf.so)."""
+    from pbf_b200 import scenes
+    V, F = scenes.icosphere(subdiv, 0.2, (0.8, 0.3, 0.5))
+    R = O.RefSDF(V, F, cell)
+    rdims, rorg, _ = R.info()
+    m, dims, org = _orc_mesh(V, F, cell)
+    try:
+        assert np.array_equal(dims, rdims) and np.array_equal(org, rorg)
+        assert np.array_equal(_orc_grid(m, dims), R.grid())
+        V2 = V + np.random.default_rng(subdiv).normal(0, 0.004, V.shape)
+        R.refit(V2)
+        O.lib().orc_mesh_refit(m, np.ascontiguousarray(V2, np.float64).reshape(-1))
+        assert np.array_equal(_orc_grid(m, dims), R.grid())
+    finally:
+        O.lib().orc_mesh_free(m)
