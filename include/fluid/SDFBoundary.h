@@ -41,6 +41,9 @@ public:
     SDFBoundary(const SDFBoundary&) = delete;
     SDFBoundary& operator=(const SDFBoundary&) = delete;
 
+    // A build of the same faces at the same resolution as the last one (the
+    // reference's periodic rebuild of a deforming mesh, main.cpp:326) runs
+    // entirely on the GPU: LBVH, face, edge and vertex pseudo-normals, grid.
     void buildFromMesh(const std::vector<std::array<double, 3>>& verts, const std::vector<std::array<int, 3>>& faces,
                        double resolution, bool verbose = true);
     void refitFromMesh(const std::vector<std::array<double, 3>>& verts);
@@ -77,6 +80,8 @@ private:
     double _cellSize = 0.0;
     pbfdrop::Vec3i _dimensions;
     std::vector<std::array<double, 3>> _buildVerts;
+    std::vector<std::array<int, 3>> _buildFaces;
+    double _buildResolution = 0.0;
     mutable std::vector<float> _distances;
     mutable bool _distancesStale = true;
 };

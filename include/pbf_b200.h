@@ -194,6 +194,14 @@ int pbf_sample_sdf(pbf_handle* h, const float* pts3, uint32_t n, float* out_d,
  *      becomes the active SDF of the handle. */
 int pbf_set_sdf_mesh(pbf_handle* h, const double* verts, int32_t nv, const int32_t* faces,
                      int32_t nf, double cell_size);
+/* buildFromMesh again for moved vertices of the faces and cell size of the
+ * last pbf_set_sdf_mesh (the reference's periodic full rebuild of a deforming
+ * mesh, src/main.cpp:326): new grid origin and dimensions from the moved
+ * bounding box, a new LBVH, face normals and the edge and angle-weighted
+ * vertex pseudo-normals recomputed, the grid recomputed, all on the GPU (the
+ * face-list adjacency from the first build is reused).  Same result as
+ * pbf_set_sdf_mesh with these vertices. */
+int pbf_rebuild_mesh(pbf_handle* h, const double* verts, int32_t nv);
 /* Moved vertices, same topology: GPU LBVH refit + face-normal refresh + full
  * grid recompute (edge/vertex pseudo-normals keep their build-time values,
  * SDFBoundary.h:58-62). */

@@ -252,6 +252,65 @@ __global__ void k_lbvh_refit(MeshDev M)
     }
 }
 
+// ---- pseudo-normals (SDFBoundary.cpp:341-383), from the current face normals --------------
+// Angle-weighted vertex normals: each incident face's normal weighted by its
+// interior angle at the vertex, summed in ascending face order (the order of
+// the reference's loop over faces), then normalised if longer than 1e-12.
+// vfc[voff[v] .. voff[v+1]) lists (face, corner) of vertex v by face.
+__global__ void k_vertex_normals(int nv, const int3* __restrict__ faces, const float3* __restrict__ verts,
+                                 const float3* __restrict__ fn, const int* __restrict__ voff,
+                                 const int2* __restrict__ vfc, float3* __restrict__ vn)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nv) return;
+    float3 s = make_float3(0.f, 0.f, 0.f);
+    for (int k = voff[v]; k < voff[v + 1]; ++k) {
+        const int2 e = vfc[k];
+        const int3 t = faces[e.x];
+        const int idx[3] = {t.x, t.y, t.z};
+        const float3 p = verts[idx[e.y]];
+        float3 a = f3sub(verts[idx[e.y == 0 ? 1 : 0]], p), b = f3sub(verts[idx[e.y == 2 ? 1 : 2]], p);
+        const float la = sqrtf(f3dot(a, a)), lb = sqrtf(f3dot(b, b));
+        if (la > 0.f) a = make_float3(a.x / la, a.y / la, a.z / la);
+        if (lb > 0.f) b = make_float3(b.x / lb, b.y / lb, b.z / lb);
+        const float ang = acosf(fminf(1.f, fmaxf(-1.f, f3dot(a, b))));
+        const float3 n = fn[e.x];
+        s = make_float3(s.x + ang * n.x, s.y + ang * n.y, s.z + ang * n.z);
+    }
+    const float len = sqrtf(f3dot(s, s));
+    if (len > 1e-12f) s = make_float3(s.x / len, s.y / len, s.z / len);
+    vn[v] = s;
+}
+
+// Edge normals: for slot 3f + k (edges AB, AC, BC of face f), the normalised
+// sum of the two face normals of an edge shared by exactly two faces
+// (partner = the other face, -1 otherwise); the face normal when there is
+// no partner or the sum is shorter than 1e-12 (a 180-degree fold).
+__global__ void k_edge_normals(int nf, const float3* __restrict__ fn, const int* __restrict__ partner,
+                               float3* __restrict__ en)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 3 * nf) return;
+    const int f = i / 3, q = partner[i];
+    float3 n = fn[f];
+    if (q >= 0) {
+        const float3 o = fn[q];
+        const float3 sm = make_float3(n.x + o.x, n.y + o.y, n.z + o.z);
+        const float len = sqrtf(f3dot(sm, sm));
+        if (len >= 1e-12f) n = make_float3(sm.x / len, sm.y / len, sm.z / len);
+    }
+    en[i] = n;
+}
+
+void launch_mesh_pseudo_normals(MeshDev M, const int* voff, const int2* vfc, const int* partner, float3* vert_n,
+                                float3* edge_n, cudaStream_t st, uint64_t* launches)
+{
+    if (M.nf <= 0) return;
+    k_vertex_normals<<<(M.nv + 127) / 128, 128, 0, st>>>(M.nv, M.faces, M.verts, M.face_n, voff, vfc, vert_n);
+    k_edge_normals<<<(3 * M.nf + 127) / 128, 128, 0, st>>>(M.nf, M.face_n, partner, edge_n);
+    if (launches) *launches += 2;
+}
+
 void launch_mesh_refit(MeshDev M, cudaStream_t st, uint64_t* launches)
 {
     if (M.nf <= 0) return;

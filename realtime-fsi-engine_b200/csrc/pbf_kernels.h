@@ -234,6 +234,12 @@ struct MeshDev {
 };
 constexpr int kMeshFrontier = 32;  // one per lane of the grid kernel's warp
 void launch_mesh_refit(MeshDev M, cudaStream_t st, uint64_t* launches);
+// Vertex (angle-weighted) and edge pseudo-normals from M.face_n (run after
+// launch_mesh_refit).  voff/vfc: per-vertex (face, corner) lists in face
+// order; partner: per face edge slot (AB, AC, BC) the other face of an edge
+// shared by exactly two faces, else -1.
+void launch_mesh_pseudo_normals(MeshDev M, const int* voff, const int2* vfc, const int* partner, float3* vert_n,
+                                float3* edge_n, cudaStream_t st, uint64_t* launches);
 void launch_mesh_grid_d(MeshDev M, int dx, int dy, int dz, const double* origin, double cell, float* out, int sms,
                         cudaStream_t st);
 void launch_morton(int nf, const int3* faces, const float3* verts, float3 lo, float3 inv_ext, uint32_t* codes,

@@ -1,14 +1,19 @@
 // pbf_mesh.cu — triangle-mesh SDF entry points of the C ABI.
 //
 // pbf_set_sdf_mesh      = SDFBoundary::buildFromMesh   (SDFBoundary.cpp:278-398)
+// pbf_rebuild_mesh      = buildFromMesh again for moved vertices of the same faces
 // pbf_update_mesh_vertices = SDFBoundary::refitFromMesh (SDFBoundary.cpp:455-465)
 // pbf_closest_triangle  = SDFBoundary::closestTriangle  (SDFBoundary.cpp:600-610)
 // pbf_vertex_forces     = computeContactForces          (src/main.cpp:604-710)
 //
-// The grid geometry (origin = bbox - 5 cells, dims = ceil(span / cell)) and the
-// edge / angle-weighted vertex pseudo-normals are computed on the host in
-// double precision at build time, exactly when the reference computes them;
-// the LBVH, face normals, node boxes, distance grid and forces live on the GPU.
+// The host derives only what depends on the face list: per-vertex (face,
+// corner) lists and each face edge's partner face (integer adjacency, once per
+// face list), and the grid geometry (origin = bbox - 5 cells, dims =
+// ceil(span / cell)) from the vertex bounding box.  Everything that depends
+// on vertex positions runs on the GPU: the LBVH build and refit, face normals,
+// the angle-weighted vertex and edge pseudo-normals, the distance grid and the
+// forces.  A build computes the pseudo-normals; a refit keeps them, as the
+// reference does (SDFBoundary.h:58-62).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -34,6 +39,10 @@ namespace {
 struct MeshHost {
     std::vector<int3> faces;
     std::vector<float3> verts_f;
+    // face-list adjacency (see build_adjacency)
+    int* d_voff = nullptr;
+    int2* d_vfc = nullptr;
+    int* d_partner = nullptr;
     // device allocations
     int3* d_faces = nullptr;
     float3* d_verts = nullptr;
@@ -54,12 +63,6 @@ struct MeshHost {
 struct D3 {
     double x, y, z;
 };
-inline D3 sub(D3 a, D3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
-inline D3 add(D3 a, D3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
-inline D3 scl(D3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
-inline double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-inline D3 cross(D3 a, D3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
-inline double norm(D3 a) { return std::sqrt(dot(a, a)); }
 
 template <class T>
 void dfree(T*& p)
@@ -88,6 +91,7 @@ void free_mesh_host(MeshHost* m)
     dfree(m->d_child); dfree(m->d_parent); dfree(m->d_bmin); dfree(m->d_bmax); dfree(m->d_leaf_face);
     dfree(m->d_flags); dfree(m->d_codes); dfree(m->d_ka); dfree(m->d_ia); dfree(m->d_kb); dfree(m->d_ib);
     dfree(m->d_hist); dfree(m->d_tot); dfree(m->d_frontier);
+    dfree(m->d_voff); dfree(m->d_vfc); dfree(m->d_partner);
     delete m;
 }
 
@@ -127,6 +131,54 @@ std::vector<int> mesh_frontier(const std::vector<int2>& child, int nf)
     return fr;
 }
 
+// Adjacency of a face list (SDFBoundary.cpp:341-383 walks the same
+// relations): for every vertex its (face, corner) incidences in ascending
+// face order, and for every face edge slot (AB, AC, BC) the other face of an
+// edge that exactly two face slots share (-1 otherwise).  The slot an edge
+// lands in follows the reference's test order: AB if it matches, else AC,
+// else BC.
+void build_adjacency(const int32_t* faces, int32_t nv, int32_t nf, std::vector<int>& voff, std::vector<int2>& vfc,
+                     std::vector<int>& partner)
+{
+    voff.assign((size_t)nv + 1, 0);
+    for (int64_t i = 0; i < 3 * (int64_t)nf; ++i) ++voff[(size_t)faces[i] + 1];
+    for (int32_t v = 0; v < nv; ++v) voff[(size_t)v + 1] += voff[(size_t)v];
+    vfc.resize(3 * (size_t)nf);
+    std::vector<int> cur(voff.begin(), voff.end() - 1);
+    for (int32_t f = 0; f < nf; ++f)
+        for (int c = 0; c < 3; ++c) vfc[(size_t)cur[(size_t)faces[3 * f + c]]++] = make_int2(f, c);
+    struct E {
+        int a, b, t;
+    };
+    std::vector<E> edges;
+    edges.reserve(3 * (size_t)nf);
+    for (int32_t f = 0; f < nf; ++f) {
+        const int A = faces[3 * f], B = faces[3 * f + 1], C = faces[3 * f + 2];
+        edges.push_back({std::min(A, B), std::max(A, B), f});
+        edges.push_back({std::min(A, C), std::max(A, C), f});
+        edges.push_back({std::min(B, C), std::max(B, C), f});
+    }
+    std::sort(edges.begin(), edges.end(), [](const E& x, const E& y) {
+        return x.a != y.a ? x.a < y.a : (x.b != y.b ? x.b < y.b : x.t < y.t);
+    });
+    partner.assign(3 * (size_t)nf, -1);
+    for (size_t i = 0; i < edges.size();) {
+        size_t j = i;
+        while (j < edges.size() && edges[j].a == edges[i].a && edges[j].b == edges[i].b) ++j;
+        if (j - i == 2) {
+            for (size_t k = i; k < j; ++k) {
+                const int t = edges[k].t, a = edges[k].a, b = edges[k].b;
+                const int A = faces[3 * t], B = faces[3 * t + 1], C = faces[3 * t + 2];
+                const int slot = (std::min(A, B) == a && std::max(A, B) == b)   ? 0
+                                 : (std::min(A, C) == a && std::max(A, C) == b) ? 1
+                                                                                : 2;
+                partner[3 * (size_t)t + slot] = edges[k == i ? i + 1 : i].t;
+            }
+        }
+        i = j;
+    }
+}
+
 }  // namespace
 
 void pbf_handle::mesh_free()
@@ -153,18 +205,16 @@ static int validate_mesh(const double* verts, int32_t nv, const int32_t* faces, 
     return PBF_OK;
 }
 
-extern "C" int pbf_set_sdf_mesh(pbf_handle* h, const double* verts, int32_t nv, const int32_t* faces, int32_t nf,
-                                double cell)
+// Everything of a build that depends on vertex positions, for the face list
+// already on the device: grid geometry from the bounding box
+// (SDFBoundary.cpp:291-308), the LBVH over Morton codes of the face
+// centroids, its subtree frontier, node boxes and face normals, the vertex
+// and edge pseudo-normals, the distance grid.
+static int mesh_build_geometry(pbf_handle* h, const double* verts, double cell)
 {
-    if (!h) return set_error(PBF_ERR_INVALID, "null handle");
-    CK(cudaSetDevice(h->device));
-    int rc = validate_mesh(verts, nv, faces, nf);
-    if (rc) return rc;
-    if (!(cell > 0.0)) return set_error(PBF_ERR_INVALID, "cell size must be > 0");
-    CK(cudaStreamSynchronize(h->stream));
-    h->mesh_free();
-
-    // grid geometry (SDFBoundary.cpp:291-308)
+    MeshHost* m = static_cast<MeshHost*>(h->mesh_host);
+    MeshDev& M = h->mesh;
+    const int nv = M.nv, nf = M.nf;
     D3 bmin{1e30, 1e30, 1e30}, bmax{-1e30, -1e30, -1e30};
     for (int i = 0; i < nv; ++i) {
         bmin = {std::min(bmin.x, verts[3 * i]), std::min(bmin.y, verts[3 * i + 1]), std::min(bmin.z, verts[3 * i + 2])};
@@ -178,97 +228,11 @@ extern "C" int pbf_set_sdf_mesh(pbf_handle* h, const double* verts, int32_t nv, 
     const size_t total = (size_t)dims[0] * dims[1] * dims[2];
     if (total == 0 || total > ((size_t)1 << 31)) return set_error(PBF_ERR_INVALID, "SDF grid of %zu voxels", total);
 
-    // pseudo-normals at build time (SDFBoundary.cpp:322-383)
-    auto V = [&](int i) { return D3{verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]}; };
-    std::vector<D3> fn(nf);
-    for (int f = 0; f < nf; ++f) {
-        D3 n = cross(sub(V(faces[3 * f + 1]), V(faces[3 * f])), sub(V(faces[3 * f + 2]), V(faces[3 * f])));
-        const double len = norm(n);
-        if (len > 1e-12) n = scl(n, 1.0 / len);
-        fn[f] = n;
-    }
-    std::vector<D3> vn(nv, D3{0, 0, 0});
-    for (int f = 0; f < nf; ++f) {
-        const int iv[3] = {faces[3 * f], faces[3 * f + 1], faces[3 * f + 2]};
-        for (int c = 0; c < 3; ++c) {
-            const D3 vtx = V(iv[c]);
-            D3 a = sub(V(iv[(c + 1) % 3]), vtx), b = sub(V(iv[(c + 2) % 3]), vtx);
-            const double la = norm(a), lb = norm(b);
-            if (la > 0) a = scl(a, 1.0 / la);
-            if (lb > 0) b = scl(b, 1.0 / lb);
-            const double cs = std::min(1.0, std::max(-1.0, dot(a, b)));
-            vn[iv[c]] = add(vn[iv[c]], scl(fn[f], std::acos(cs)));
-        }
-    }
-    for (auto& n : vn) {
-        const double len = norm(n);
-        if (len > 1e-12) n = scl(n, 1.0 / len);
-    }
-    std::vector<D3> en(3 * (size_t)nf);
-    for (int f = 0; f < nf; ++f) en[3 * f] = en[3 * f + 1] = en[3 * f + 2] = fn[f];
-    struct E {
-        int a, b, t;
-    };
-    std::vector<E> edges;
-    edges.reserve(3 * (size_t)nf);
-    for (int f = 0; f < nf; ++f) {
-        const int A = faces[3 * f], B = faces[3 * f + 1], C = faces[3 * f + 2];
-        edges.push_back({std::min(A, B), std::max(A, B), f});
-        edges.push_back({std::min(A, C), std::max(A, C), f});
-        edges.push_back({std::min(B, C), std::max(B, C), f});
-    }
-    std::sort(edges.begin(), edges.end(), [](const E& x, const E& y) {
-        return x.a != y.a ? x.a < y.a : (x.b != y.b ? x.b < y.b : x.t < y.t);
-    });
-    for (size_t i = 0; i < edges.size();) {
-        size_t j = i;
-        while (j < edges.size() && edges[j].a == edges[i].a && edges[j].b == edges[i].b) ++j;
-        if (j - i == 2) {
-            const D3 s = add(fn[edges[i].t], fn[edges[i + 1].t]);
-            const double len = norm(s);
-            if (len >= 1e-12) {
-                const D3 e = scl(s, 1.0 / len);
-                for (size_t k = i; k < j; ++k) {
-                    const int t = edges[k].t, a = edges[k].a, b = edges[k].b;
-                    const int A = faces[3 * t], B = faces[3 * t + 1], C = faces[3 * t + 2];
-                    if (std::min(A, B) == a && std::max(A, B) == b) en[3 * t] = e;
-                    else if (std::min(A, C) == a && std::max(A, C) == b) en[3 * t + 1] = e;
-                    else en[3 * t + 2] = e;
-                }
-            }
-        }
-        i = j;
-    }
-
-    MeshHost* m = new MeshHost();
-    h->mesh_host = m;
-    m->faces.resize(nf);
-    for (int f = 0; f < nf; ++f) m->faces[f] = make_int3(faces[3 * f], faces[3 * f + 1], faces[3 * f + 2]);
-    m->verts_f.resize(nv);
-    for (int i = 0; i < nv; ++i) m->verts_f[i] = make_float3((float)verts[3 * i], (float)verts[3 * i + 1], (float)verts[3 * i + 2]);
-    std::vector<float3> enf(3 * (size_t)nf), vnf(nv);
-    for (size_t i = 0; i < enf.size(); ++i) enf[i] = make_float3((float)en[i].x, (float)en[i].y, (float)en[i].z);
-    for (int i = 0; i < nv; ++i) vnf[i] = make_float3((float)vn[i].x, (float)vn[i].y, (float)vn[i].z);
-
-    const size_t nodes = 2 * (size_t)nf - 1;
-    if ((rc = dalloc(m->d_faces, nf)) || (rc = dalloc(m->d_verts, nv)) || (rc = dalloc(m->d_face_n, nf)) ||
-        (rc = dalloc(m->d_edge_n, 3 * (size_t)nf)) || (rc = dalloc(m->d_vert_n, nv)) ||
-        (rc = dalloc(m->d_child, std::max<size_t>(1, nf - 1))) || (rc = dalloc(m->d_parent, nodes)) ||
-        (rc = dalloc(m->d_bmin, nodes)) || (rc = dalloc(m->d_bmax, nodes)) || (rc = dalloc(m->d_leaf_face, nf)) ||
-        (rc = dalloc(m->d_flags, std::max<size_t>(1, nf - 1))) || (rc = dalloc(m->d_codes, nf)) ||
-        (rc = dalloc(m->d_ka, nf)) || (rc = dalloc(m->d_ia, nf)) || (rc = dalloc(m->d_kb, nf)) ||
-        (rc = dalloc(m->d_ib, nf)) || (rc = dalloc(m->d_hist, (size_t)256 * sort_num_tiles(nf))) ||
-        (rc = dalloc(m->d_tot, 256)) || (rc = dalloc(h->force_acc, 3 * (size_t)nv)) ||
-        (rc = dalloc(h->force_contacts, 1)) || (rc = dalloc(h->force_out, 3 * (size_t)nv))) {
-        h->mesh_free();
-        return rc;
-    }
+    for (int i = 0; i < nv; ++i)
+        m->verts_f[i] = make_float3((float)verts[3 * i], (float)verts[3 * i + 1], (float)verts[3 * i + 2]);
     cudaStream_t st = h->stream;
-    CK(cudaMemcpyAsync(m->d_faces, m->faces.data(), sizeof(int3) * nf, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(m->d_verts, m->verts_f.data(), sizeof(float3) * nv, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(m->d_edge_n, enf.data(), sizeof(float3) * enf.size(), cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(m->d_vert_n, vnf.data(), sizeof(float3) * nv, cudaMemcpyHostToDevice, st));
-    CK(cudaMemsetAsync(m->d_parent, 0xFF, sizeof(int) * nodes, st));
+    CK(cudaMemsetAsync(m->d_parent, 0xFF, sizeof(int) * (2 * (size_t)nf - 1), st));
 
     // LBVH: Morton codes of the face centroids over the vertex bbox
     const float3 lo = make_float3((float)bmin.x, (float)bmin.y, (float)bmin.z);
@@ -283,19 +247,71 @@ extern "C" int pbf_set_sdf_mesh(pbf_handle* h, const double* verts, int32_t nv, 
     launch_lbvh_topology(nf, sk, m->d_child, m->d_parent, st);
     h->launches += 2;
     {
-        // the grid kernel's per-lane subtrees (the topology is fixed until the next build)
+        // the grid kernel's per-lane subtrees (the tree shape is fixed until the next build)
         std::vector<int2> child(std::max(1, nf - 1), make_int2(-1, -1));
         if (nf > 1)
             CK(cudaMemcpyAsync(child.data(), m->d_child, sizeof(int2) * (size_t)(nf - 1), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         const std::vector<int> fr = mesh_frontier(child, nf);
-        if ((rc = dalloc(m->d_frontier, (size_t)kMeshFrontier))) {
-            h->mesh_free();
-            return rc;
-        }
         CK(cudaMemcpyAsync(m->d_frontier, fr.data(), sizeof(int) * kMeshFrontier, cudaMemcpyHostToDevice, st));
-        CK(cudaStreamSynchronize(st));
     }
+    launch_mesh_refit(M, st, &h->launches);
+    launch_mesh_pseudo_normals(M, m->d_voff, m->d_vfc, m->d_partner, m->d_vert_n, m->d_edge_n, st, &h->launches);
+
+    for (int a = 0; a < 3; ++a) h->origin_d[a] = o[a];
+    h->cell_d = cell;
+    const float of[3] = {(float)o[0], (float)o[1], (float)o[2]};
+    int rc;
+    if ((rc = h->upload_grid(nullptr, dims, of, (float)cell))) return rc;
+    launch_mesh_grid_d(M, dims[0], dims[1], dims[2], h->origin_d, cell, h->grid, h->num_sms, st);
+    launch_sdf_slab_min(h->grid, dims[0], dims[1], dims[2], h->slab_min, st);
+    h->launches += 2;
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    return PBF_OK;
+}
+
+extern "C" int pbf_set_sdf_mesh(pbf_handle* h, const double* verts, int32_t nv, const int32_t* faces, int32_t nf,
+                                double cell)
+{
+    if (!h) return set_error(PBF_ERR_INVALID, "null handle");
+    CK(cudaSetDevice(h->device));
+    int rc = validate_mesh(verts, nv, faces, nf);
+    if (rc) return rc;
+    if (!(cell > 0.0)) return set_error(PBF_ERR_INVALID, "cell size must be > 0");
+    CK(cudaStreamSynchronize(h->stream));
+    h->mesh_free();
+
+    std::vector<int> voff, partner;
+    std::vector<int2> vfc;
+    build_adjacency(faces, nv, nf, voff, vfc, partner);
+
+    MeshHost* m = new MeshHost();
+    h->mesh_host = m;
+    m->faces.resize(nf);
+    for (int f = 0; f < nf; ++f) m->faces[f] = make_int3(faces[3 * f], faces[3 * f + 1], faces[3 * f + 2]);
+    m->verts_f.resize(nv);
+
+    const size_t nodes = 2 * (size_t)nf - 1;
+    if ((rc = dalloc(m->d_faces, nf)) || (rc = dalloc(m->d_verts, nv)) || (rc = dalloc(m->d_face_n, nf)) ||
+        (rc = dalloc(m->d_edge_n, 3 * (size_t)nf)) || (rc = dalloc(m->d_vert_n, nv)) ||
+        (rc = dalloc(m->d_child, std::max<size_t>(1, nf - 1))) || (rc = dalloc(m->d_parent, nodes)) ||
+        (rc = dalloc(m->d_bmin, nodes)) || (rc = dalloc(m->d_bmax, nodes)) || (rc = dalloc(m->d_leaf_face, nf)) ||
+        (rc = dalloc(m->d_flags, std::max<size_t>(1, nf - 1))) || (rc = dalloc(m->d_codes, nf)) ||
+        (rc = dalloc(m->d_ka, nf)) || (rc = dalloc(m->d_ia, nf)) || (rc = dalloc(m->d_kb, nf)) ||
+        (rc = dalloc(m->d_ib, nf)) || (rc = dalloc(m->d_hist, (size_t)256 * sort_num_tiles(nf))) ||
+        (rc = dalloc(m->d_tot, 256)) || (rc = dalloc(m->d_frontier, (size_t)kMeshFrontier)) ||
+        (rc = dalloc(m->d_voff, (size_t)nv + 1)) || (rc = dalloc(m->d_vfc, 3 * (size_t)nf)) ||
+        (rc = dalloc(m->d_partner, 3 * (size_t)nf)) || (rc = dalloc(h->force_acc, 3 * (size_t)nv)) ||
+        (rc = dalloc(h->force_contacts, 1)) || (rc = dalloc(h->force_out, 3 * (size_t)nv))) {
+        h->mesh_free();
+        return rc;
+    }
+    cudaStream_t st = h->stream;
+    CK(cudaMemcpyAsync(m->d_faces, m->faces.data(), sizeof(int3) * nf, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(m->d_voff, voff.data(), sizeof(int) * voff.size(), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(m->d_vfc, vfc.data(), sizeof(int2) * vfc.size(), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(m->d_partner, partner.data(), sizeof(int) * partner.size(), cudaMemcpyHostToDevice, st));
 
     MeshDev M{};
     M.nv = nv;
@@ -313,19 +329,24 @@ extern "C" int pbf_set_sdf_mesh(pbf_handle* h, const double* verts, int32_t nv, 
     M.flags = m->d_flags;
     M.frontier = m->d_frontier;
     h->mesh = M;
-    launch_mesh_refit(M, st, &h->launches);
-
-    for (int a = 0; a < 3; ++a) h->origin_d[a] = o[a];
-    h->cell_d = cell;
-    const float of[3] = {(float)o[0], (float)o[1], (float)o[2]};
-    if ((rc = h->upload_grid(nullptr, dims, of, (float)cell))) return rc;
-    launch_mesh_grid_d(M, dims[0], dims[1], dims[2], h->origin_d, cell, h->grid, h->num_sms, st);
-    launch_sdf_slab_min(h->grid, dims[0], dims[1], dims[2], h->slab_min, st);
-    h->launches += 2;
+    if ((rc = mesh_build_geometry(h, verts, cell))) {
+        h->mesh_free();
+        return rc;
+    }
     h->mesh_attached = true;
-    CK(cudaStreamSynchronize(st));
-    CK(cudaGetLastError());
     return PBF_OK;
+}
+
+extern "C" int pbf_rebuild_mesh(pbf_handle* h, const double* verts, int32_t nv)
+{
+    if (!h) return set_error(PBF_ERR_INVALID, "null handle");
+    CK(cudaSetDevice(h->device));
+    if (!h->mesh_attached) return set_error(PBF_ERR_STATE, "no mesh attached");
+    if (!verts || nv != h->mesh.nv) return set_error(PBF_ERR_INVALID, "vertex count %d != %d", nv, h->mesh.nv);
+    for (int64_t i = 0; i < 3 * (int64_t)nv; ++i)
+        if (!std::isfinite(verts[i])) return set_error(PBF_ERR_INVALID, "non-finite vertex coordinate");
+    CK(cudaStreamSynchronize(h->stream));
+    return mesh_build_geometry(h, verts, h->cell_d);
 }
 
 extern "C" int pbf_update_mesh_vertices(pbf_handle* h, const double* verts, int32_t nv)

@@ -41,8 +41,12 @@ void SDFBoundary::buildFromMesh(const std::vector<std::array<double, 3>>& verts,
                                 const std::vector<std::array<int, 3>>& faces, double resolution, bool verbose)
 {
     if (!_h) return;
-    const int rc = pbf_set_sdf_mesh(_h, verts.empty() ? nullptr : verts[0].data(), (int32_t)verts.size(),
-                                    faces.empty() ? nullptr : faces[0].data(), (int32_t)faces.size(), resolution);
+    const bool same_faces = _valid && resolution == _buildResolution && faces == _buildFaces &&
+                            verts.size() == _buildVerts.size();
+    const int rc = same_faces ? pbf_rebuild_mesh(_h, verts[0].data(), (int32_t)verts.size())
+                              : pbf_set_sdf_mesh(_h, verts.empty() ? nullptr : verts[0].data(), (int32_t)verts.size(),
+                                                 faces.empty() ? nullptr : faces[0].data(), (int32_t)faces.size(),
+                                                 resolution);
     if (rc != PBF_OK) {
         std::fprintf(stderr, "SDFBoundary::buildFromMesh: %s\n", pbf_last_error());
         _valid = false;
@@ -50,6 +54,10 @@ void SDFBoundary::buildFromMesh(const std::vector<std::array<double, 3>>& verts,
     }
     _valid = true;
     _buildVerts = verts;
+    if (!same_faces) {
+        _buildFaces = faces;
+        _buildResolution = resolution;
+    }
     refreshInfo();
     if (verbose)
         std::printf("SDF computed: %dx%dx%d (%d voxels, %zu triangles, LBVH)\n", _dimensions.x(), _dimensions.y(),

@@ -67,6 +67,7 @@ class SDFBoundary:
         check(lib().pbf_create(C.byref(default_config()), int(device), C.byref(self._h)))
         self._nv = 0
         self._faces = None
+        self._resolution = None
         self._build_verts = None
 
     def __del__(self):
@@ -79,11 +80,19 @@ class SDFBoundary:
 
     # ---- build / refit ------------------------------------------------------
     def buildFromMesh(self, verts, faces, resolution, verbose=False):
+        """A build of the same faces at the same resolution as the last one (a
+        deforming mesh's periodic rebuild) runs entirely on the GPU
+        (pbf_rebuild_mesh); any other build starts from the face list."""
         v = np.ascontiguousarray(verts, dtype=np.float64).reshape(-1, 3)
         f = np.ascontiguousarray(faces, dtype=np.int32).reshape(-1, 3)
-        check(lib().pbf_set_sdf_mesh(self._h, _ptr(v), len(v), _ptr(f), len(f), float(resolution)))
+        if (self._faces is not None and float(resolution) == self._resolution and len(v) == self._nv
+                and np.array_equal(f, self._faces)):
+            check(lib().pbf_rebuild_mesh(self._h, _ptr(v), len(v)))
+        else:
+            check(lib().pbf_set_sdf_mesh(self._h, _ptr(v), len(v), _ptr(f), len(f), float(resolution)))
+            self._faces = f
+            self._resolution = float(resolution)
         self._nv = len(v)
-        self._faces = f
         self._build_verts = v.copy()
         if verbose:
             d = self.dimensions()

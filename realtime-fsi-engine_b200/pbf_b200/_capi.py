@@ -150,6 +150,7 @@ SIGNATURES = [
     ("pbf_read_sdf_grid", C.c_int, [vp, vp, C.c_size_t]),
     ("pbf_sample_sdf", C.c_int, [vp, vp, u32, vp, vp]),
     ("pbf_set_sdf_mesh", C.c_int, [vp, vp, i32, vp, i32, C.c_double]),
+    ("pbf_rebuild_mesh", C.c_int, [vp, vp, i32]),
     ("pbf_update_mesh_vertices", C.c_int, [vp, vp, i32]),
     ("pbf_sdf_grid_info", C.c_int, [vp, P(i32), P(C.c_double), P(C.c_double)]),
     ("pbf_closest_triangle", C.c_int, [vp, vp, u32, vp, vp]),

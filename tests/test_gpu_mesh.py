@@ -1,12 +1,13 @@
-"""Triangle-mesh SDF on the GPU (LBVH build/refit, grid, closest triangle,
-per-vertex contact forces) against the FP64 restatement of
-src/fluid/SDFBoundary.cpp and src/main.cpp:604-710.
-
-The reference's own SDFBoundary.cpp cannot be compiled here (its Eigen/Core
-is missing from the vendored tree), so this part of the oracle is a
-restatement without golden vectors; the GPU is compared with it at FP32
-tolerances, and the analytic sphere bounds both.
+"""Triangle-mesh SDF on the GPU (LBVH build/refit/rebuild, pseudo-normals,
+grid, closest triangle, per-vertex contact forces) against the FP64
+restatement of src/fluid/SDFBoundary.cpp and src/main.cpp:604-710, and
+directly against the reference's own SDFBoundary (fixture sdf_ref.npz, made
+by compiling SDFBoundary.cpp here; the restatement equals it bit for bit,
+tests/test_oracle_golden.py).  The GPU computes in FP32: grids agree within
+2e-6, the analytic sphere bounds both.
 """
+import os
+
 import ctypes as C
 
 import numpy as np
@@ -14,6 +15,7 @@ import pytest
 
 import oracle as O
 import pbf_b200 as P
+import pbfh as H
 from pbf_b200 import scenes
 
 pytestmark = pytest.mark.gpu
@@ -73,6 +75,53 @@ def test_refit_after_deformation_matches_oracle(have_gpu):
         # refitDirty reports movement beyond moveEps only
         assert sdf.refitDirty(V2 + 1e-6, 0.05, 1e-4) is False
         assert sdf.refitDirty(V2 + 1e-3, 0.05, 1e-4) is True
+    finally:
+        O.lib().orc_mesh_free(m)
+
+
+def test_build_refit_rebuild_match_reference_sdfboundary(have_gpu):
+    """The reference's own SDFBoundary on an icosphere: the GPU grid after a
+    build, after refitFromMesh of moved vertices (build-time edge and vertex
+    pseudo-normals kept) and after buildFromMesh of the moved vertices (all
+    pseudo-normals recomputed on the GPU: pbf_rebuild_mesh), and the closest
+    points at seeded queries."""
+    z = H.load("sdf_ref.npz")
+    cell = float(z["cell"])
+    sdf = P.SDFBoundary()
+    sdf.buildFromMesh(z["verts"], z["faces"], cell)
+    assert np.array_equal(sdf.dimensions(), z["dims"])
+    assert np.allclose(sdf.origin(), z["origin"], rtol=0, atol=1e-12)
+    assert np.abs(sdf.distances() - z["grid"]).max() < 2e-6
+    _, point = sdf.closest_many(z["query"])
+    assert np.abs(point - z["closest_point"]).max() < 2e-6
+    sdf.refitFromMesh(z["verts_moved"])
+    assert np.abs(sdf.distances() - z["refit_grid"]).max() < 2e-6
+    sdf.buildFromMesh(z["verts_moved"], z["faces"], cell)  # same faces: the GPU rebuild
+    assert np.array_equal(sdf.dimensions(), z["rebuild_dims"])
+    assert np.allclose(sdf.origin(), z["rebuild_origin"], rtol=0, atol=1e-12)
+    assert np.abs(sdf.distances() - z["rebuild_grid"]).max() < 2e-6
+
+
+def test_gpu_rebuild_equals_fresh_build(have_gpu):
+    """pbf_rebuild_mesh (moved vertices, cached face adjacency) gives the grid
+    a fresh pbf_set_sdf_mesh of the moved mesh gives, bit for bit, including
+    new grid dimensions when the bounding box grows."""
+    V, F = scenes.icosphere(4, 0.2, (0.8, 0.3, 0.5))
+    rng = np.random.default_rng(9)
+    V2 = V + rng.normal(0, 0.003, V.shape)
+    V2[V2[:, 1] > 0.45] += [0.0, 0.05, 0.0]  # the top pulled up: a taller box
+    a = P.SDFBoundary()
+    a.buildFromMesh(V, F, 0.0125)
+    d0 = a.dimensions()
+    a.buildFromMesh(V2, F, 0.0125)
+    b = P.SDFBoundary()
+    b.buildFromMesh(V2, F, 0.0125)
+    assert not np.array_equal(a.dimensions(), d0)
+    assert np.array_equal(a.dimensions(), b.dimensions())
+    assert np.array_equal(a.distances(), b.distances())
+    m, dims, _ = oracle_mesh(V2, F, 0.0125)
+    try:
+        assert np.abs(a.distances() - oracle_grid(m, dims)).max() < 2e-6
     finally:
         O.lib().orc_mesh_free(m)
 
