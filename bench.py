@@ -57,12 +57,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="c2 only: skip the short C3 batch and C4 adjoint runs attached to the line")
-    ap.add_argument("--mode", type=int, default=-1, choices=[-1, 0, 1, 2, 3, 4, 5, 6, 7, 8],
-                    help="neighbour passes: -1 automatic (default: 8 from 2^19 particles, else 4), 0 hash order, "
-                         "1 Morton, 2 Morton cell-cooperative, 3 Morton with per-lane pair queues, 4 Morton with "
-                         "per-bucket hit masks, 5 Morton cell blocks staged through shared memory, 6 neighbour "
-                         "lists with a skin, 7 per-block dense cell box in shared memory, 8 x-runs of a dense cell "
-                         "window")
+    ap.add_argument("--mode", type=int, default=-1, choices=[-1, 4, 8],
+                    help="neighbour passes: -1 automatic (default: 8 from 2^19 particles, else 4), 4 hashed "
+                         "buckets in Morton thread order with per-bucket hit masks, 8 x-runs of a dense cell window")
     ap.add_argument("--sample", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
                     help="smaller lattice of the same scene (profiling captures only)")
     return ap.parse_args()
@@ -312,7 +309,7 @@ def run_b200(args, dist):
     clocks = Clocks(dev)
     l0 = fl.kernel_launches()
     mode = args.mode if args.mode >= 0 else (8 if n >= (1 << 19) else 4)
-    ws0 = fl.list_stats() if mode in (6, 7, 8) else None
+    ws0 = fl.list_stats() if mode == 8 else None
     e0.record(stream)
     for _ in range(args.steps):
         fl.step()
@@ -398,7 +395,7 @@ def run_b200(args, dist):
             "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
             "passes": per_pass, "nonfinite_particles": int(bad), "impl": "b200"}
     if ws1 is not None:
-        # pbf_list_stats before and after the timed steps (meaning per mode in pbf_b200.h)
+        # pbf_list_stats before and after the timed steps (bucket walks, drift marks, unclean cells)
         line["walk_stats"] = {"before": list(ws0), "after": list(ws1)}
     del fl, obstacle
     if args.workload == "c2" and not args.no_extras and not args.sample:

@@ -296,29 +296,11 @@ int pbf_kernel_launches(pbf_handle* h, uint64_t* out);
  * parameter, particle or SDF change). */
 int pbf_set_use_graph(pbf_handle* h, int on);
 /* Execution options (results do not depend on them; no reference counterpart):
- *   PBF_OPT_SPATIAL_ORDER  -1 (default): mode 8 from 2^19 particles, mode 4
- *                          below (where mode 8's relabelling launches cost
- *                          more than its walk saves).  4: neighbour passes
- *                          take particles in the Morton order of their cells,
- *                          one thread each, and test each bucket in chunks of
- *                          8 before running the pair body on the hits (the
- *                          mode APBF and windows over 2^26 cells run under
- *                          modes 6 and 8); 1: Morton order, body inside
- *                          the candidate loop; 2: Morton order, one warp per
- *                          cell with lanes sharing the candidate walk;
- *                          3: Morton order, in-range pairs queued per lane and
- *                          drained warp-wide; 5: Morton order, the distinct
- *                          buckets of each 256-particle block staged once in
- *                          shared memory (falls back to global reads when a
- *                          block's buckets exceed the stage); 0: hash order.
- *                          6: Morton-labelled data and per-substep neighbour
- *                          lists built in the first lambda pass with a skin
- *                          (PBF_OPT_LIST_SKIN); later passes walk the list
- *                          where it provably yields the bucket walk's hits
- *                          and walk the buckets elsewhere (APBF runs mode 4);
- *                          7: Morton order, each 256-particle block stages the
- *                          buckets of its widened cell box in shared memory
- *                          (dense cell table) and walks them there.
+ *   PBF_OPT_SPATIAL_ORDER  the neighbour passes' walk.
+ *                          4: particles taken in the Morton order of their
+ *                          cells, one thread each, each of the 27 hashed
+ *                          buckets tested in chunks of 8 before the pair body
+ *                          runs on the hits.
  *                          8: data relabelled by the slot of each particle's
  *                          cell in a dense window of the box (z, y, x), so
  *                          the three x-adjacent cells of a row are one label
@@ -327,24 +309,20 @@ int pbf_set_use_graph(pbf_handle* h, int on);
  *                          particle within reach has moved 0.9 h since the
  *                          predict near a colliding cell; the hashed buckets
  *                          elsewhere.  Same pairs, same order as the buckets.
- *                          Modes 4, 6 and 8 give bit-identical results (same
- *                          pairs, order and pair arithmetic); the others the
- *                          same up to FP32 summation-order and contraction
- *                          differences.
- *   PBF_OPT_LIST_SKIN      mode 6 list reach beyond h, in 1/1000 h (default 100). */
+ *                          -1 (default): mode 8 from 2^19 particles, mode 4
+ *                          below (where mode 8's relabelling launches cost
+ *                          more than its walk saves); APBF and windows over
+ *                          2^26 cells run mode 4.  Modes 4 and 8 give
+ *                          bit-identical results (same pairs, order and pair
+ *                          arithmetic).  Other values: PBF_ERR_INVALID. */
 #define PBF_OPT_SPATIAL_ORDER 1
-#define PBF_OPT_LIST_SKIN 2
 int pbf_set_option(pbf_handle* h, int option, int value);
 
-/* Mode 6 statistics of the last substep, summed over its passes: particles
- * that walked all 27 buckets instead of their list (moved more than skin/2
- * or changed cell), marked buckets walked in full from a list, and buckets
- * marked because one of their particles moved more than skin/2.
- * Mode 7: blocks and particles that walked global memory (since creation).
- * Mode 8: particle passes that walked the hashed buckets (since the window was
- * set up), particles beyond the 0.9 h drift bound that marked the cells within
- * their reach in the last substep (a same-bucket cell was near; counted per
- * pass), and window cells whose neighbourhood has a hash collision. */
+/* Mode 8 statistics: particle passes that walked the hashed buckets (since
+ * the window was set up), particles beyond the 0.9 h drift bound that marked
+ * the cells within their reach in the last substep (a same-bucket cell was
+ * near; counted per pass), and window cells whose neighbourhood has a hash
+ * collision.  Zeros in mode 4. */
 int pbf_list_stats(pbf_handle* h, uint32_t* full_walks, uint32_t* bucket_walks, uint32_t* marked_buckets);
 
 /* ---- health ------------------------------------------------------------- */

@@ -646,6 +646,22 @@ __device__ __forceinline__ void mark_moved(const DevParams& P, const DenseArgs& 
             }
 }
 
+// Label-order arrays gathered back into hash-sorted order (slot s <- label
+// inv[s]) for the buffer reads of the stage-level API.
+__global__ void k_d_unpermute4(uint32_t n, const uint32_t* __restrict__ inv, const float4* __restrict__ src,
+                               float4* __restrict__ dst)
+{
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += stride) dst[s] = __ldg(src + __ldg(inv + s));
+}
+
+__global__ void k_d_unpermute1(uint32_t n, const uint32_t* __restrict__ inv, const float* __restrict__ src,
+                               float* __restrict__ dst)
+{
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += stride) dst[s] = __ldg(src + __ldg(inv + s));
+}
+
 // ---- thread order by current cell ----------------------------------------------------------
 // The labels follow the predict-time cells; once the corrections have moved
 // particles, consecutive labels query different current cells and a warp's
@@ -1053,5 +1069,17 @@ void launch_d_vorticity(const DevParams& P, const DenseArgs& D, const float4* lx
 }
 
 #undef PBF_DENSE_LAUNCH
+
+void launch_d_unpermute4(uint32_t n, const uint32_t* inv, const float4* src, float4* dst, int sms, cudaStream_t st)
+{
+    const uint32_t want = (n + 255u) / 256u, cap = (uint32_t)sms * 8u;
+    k_d_unpermute4<<<want < 1 ? 1 : (want > cap ? cap : want), 256, 0, st>>>(n, inv, src, dst);
+}
+
+void launch_d_unpermute1(uint32_t n, const uint32_t* inv, const float* src, float* dst, int sms, cudaStream_t st)
+{
+    const uint32_t want = (n + 255u) / 256u, cap = (uint32_t)sms * 8u;
+    k_d_unpermute1<<<want < 1 ? 1 : (want > cap ? cap : want), 256, 0, st>>>(n, inv, src, dst);
+}
 
 }  // namespace pbf

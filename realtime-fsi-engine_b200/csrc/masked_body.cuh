@@ -1,16 +1,16 @@
 // masked_body.cuh — per-particle bodies of the neighbour passes, shared by
-// the single-scene kernels (k_masked.cu, k_list.cu), the multi-scene kernels
-// (k_batch.cu) and the adjoint's recording passes (k_adjoint.cu), so that
-// all of them run the same arithmetic on every pair.
+// the single-scene kernels (k_masked.cu, k_dense.cu), the multi-scene kernels
+// (k_batch.cu, k_dense.cu) and the adjoint's recording passes (k_adjoint.cu),
+// so that all of them run the same arithmetic on every pair.
 //
 // Each pass is a `*_core` function parameterised by a walker: walk(hit, body)
 // calls body(k) for every candidate k with hit(r^2) true, in the reference's
 // visiting order (CS_ComputeLambdas.glsl:126-150: 27 hashed buckets, z outer,
 // x inner, bucket contents in sorted order, colliding buckets once per
 // neighbour cell), where k indexes the position array X the core reads
-// neighbours from.  Two walkers exist: masked_walk below (the hashed buckets
-// themselves) and the neighbour-list walk of k_list.cu (the same candidate
-// sequence, pre-filtered).
+// neighbours from.  The walkers: masked_walk below (the hashed buckets
+// themselves) and the run and bucket walks of k_dense.cu (the same hits in
+// the same order over the relabelled arrays).
 //
 // masked_walk: for each bucket, up to 8 candidates are loaded with
 // independent predicated loads and reduced to an 8-bit mask of hits; the

@@ -274,9 +274,7 @@ int pbf_handle::ensure_capacity(uint32_t need_n)
         const size_t c = need_n;
         if ((rc = dalloc(pos, c)) || (rc = dalloc(vel, c)) || (rc = dalloc(pred, c)) || (rc = dalloc(aos, 3 * c)) ||
             (rc = dalloc(keys, c)) || (rc = dalloc(ka, c)) || (rc = dalloc(mcode, c)) || (rc = dalloc(mka, c)) ||
-            (rc = dalloc(mia, c)) || (rc = dalloc(mkb, c)) || (rc = dalloc(mib, c)) ||
-            (rc = dalloc(run_starts, c + 1)) || (rc = dalloc(run_blocks, (size_t)head_num_blocks(need_n) + 1)) ||
-            (rc = dalloc(ia, c)) || (rc = dalloc(kb, c)) || (rc = dalloc(ib, c)) || (rc = dalloc(sx[0], c)) ||
+            (rc = dalloc(mia, c)) || (rc = dalloc(mkb, c)) || (rc = dalloc(mib, c)) || (rc = dalloc(ia, c)) || (rc = dalloc(kb, c)) || (rc = dalloc(ib, c)) || (rc = dalloc(sx[0], c)) ||
             (rc = dalloc(sx[1], c)) || (rc = dalloc(sv, c)) || (rc = dalloc(sx0, c)) || (rc = dalloc(somega, c)) ||
             (rc = dalloc(rho, c)) || (rc = dalloc(lod, c)) || (rc = dalloc(cand, 2 * c)) ||
             (rc = dalloc(ct_counts, (size_t)contact_num_blocks(need_n) + 1)))
@@ -312,11 +310,11 @@ pbf_handle::~pbf_handle()
     }
     for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
     dfree(pos); dfree(vel); dfree(pred); dfree(aos); dfree(keys);
-    dfree(mcode); dfree(mka); dfree(mia); dfree(mkb); dfree(mib); dfree(run_starts); dfree(run_blocks); dfree(ka); dfree(ia); dfree(kb); dfree(ib);
+    dfree(mcode); dfree(mka); dfree(mia); dfree(mkb); dfree(mib); dfree(ka); dfree(ia); dfree(kb); dfree(ib);
     dfree(sx[0]); dfree(sx[1]); dfree(sv); dfree(sx0); dfree(somega); dfree(rho); dfree(lod);
     dfree(hist); dfree(totals); dfree(table); dfree(cand); dfree(ct_counts); dfree(scalars);
     dfree(lx[0]); dfree(lx[1]); dfree(lxb); dfree(lv); dfree(lx0); dfree(lom); dfree(lrho);
-    dfree(lid); dfree(lkey); dfree(inv); dfree(list); dfree(lcnt); dfree(lstats); dfree(fastb);
+    dfree(lid); dfree(lkey); dfree(inv);
     dfree(dtable); dfree(druns); dfree(dclean); dfree(ddcol); dfree(ddirty); dfree(dflag);
     dfree(dslot); dfree(dord); dfree(dcnt); dfree(dbsum); dfree(dhm); dfree(dhcnt); dfree(dvmark);
     dfree(grid); dfree(slab_min);
@@ -376,18 +374,17 @@ int pbf_handle::prof_collect()
     return PBF_OK;
 }
 
-// ---- neighbour lists (mode 6) ---------------------------------------------------------
-// Mode 6 needs every iteration to run (no APBF skips) and one displacement
-// slot per moving pass; otherwise the handle runs mode 4.
-// Mode 8 likewise (label arrays without APBF's per-particle skips), and only
-// when the dense window of the box stays within 2^26 cells.
-// Automatic choice (the default, pass_mode < 0): mode 8 from 2^19 particles,
-// below which its extra relabelling launches cost more than its walk saves
-// (measured crossover between 2.6e5 and 8.8e5 particles), mode 4 below.
+// ---- neighbour-pass mode -----------------------------------------------------------------
+// Mode 8 (dense-window runs) needs label arrays without APBF's per-particle
+// skips and a dense window of the box within 2^26 cells; otherwise the
+// handle runs mode 4 (hashed buckets).  Automatic choice (the default,
+// pass_mode < 0): mode 8 from 2^19 particles, below which its extra
+// relabelling launches cost more than its walk saves (measured crossover
+// between 2.6e5 and 8.8e5 particles), mode 4 below.
 int pbf_handle::effective_mode() const
 {
     const int mode = pass_mode >= 0 ? pass_mode : (n >= (1u << 19) ? 8 : 4);
-    if ((mode == 6 || mode == 8) && (derived.enable_apbf || n >= (1u << 27))) return 4;
+    if (mode == 8 && (derived.enable_apbf || n >= (1u << 27))) return 4;
     if (mode == 8) {
         int g0[3];
         uint32_t nd[3];
@@ -515,56 +512,23 @@ int pbf_handle::ensure_dense()
     return PBF_OK;
 }
 
-int pbf_handle::ensure_list_capacity()
-{
-    int rc;
-    if ((rc = ensure_label_capacity())) return rc;
-    if (cap_list_n < n || !list) {
-        const size_t c = std::max<uint32_t>(n, 1u);
-        if ((rc = dalloc(list, c * list_cap)) || (rc = dalloc(lcnt, c)) || (rc = dalloc(lstats, 4))) return rc;
-        cap_list_n = (uint32_t)c;
-    }
-    if (cap_fast != derived.hash_size || !fastb) {
-        if ((rc = dalloc(fastb, derived.hash_size))) return rc;
-        cap_fast = derived.hash_size;
-    }
-    return PBF_OK;
-}
-
-ListArgs pbf_handle::list_args() const
-{
-    ListArgs A;
-    A.table = table;
-    A.inv = inv;
-    A.list = list;
-    A.cnt = lcnt;
-    A.xb = lxb;
-    A.lkey = lkey;
-    A.fastb = fastb;
-    A.stats = lstats;
-    // margin 1e-4 h absorbs the FP32 rounding of the distances compared
-    const float hs = (0.5f * list_skin - 1e-4f) * derived.h;
-    A.half_skin2 = hs > 0.0f ? hs * hs : 0.0f;
-    return A;
-}
-
-// Sorted-order buffers are kept in label order in modes 6 and 8: gather the one
-// asked for back into sorted (hash) order before it is read.
+// Sorted-order buffers are kept in label order in mode 8: gather the one asked
+// for back into sorted (hash) order before it is read.
 int pbf_handle::unpermute_for_read(int which)
 {
     if (!label_space) return PBF_OK;
     switch (which) {
     case PBF_BUF_XSTAR:
-        launch_l_unpermute4(n, inv, lx[last_x], sx[last_x], num_sms, stream);
+        launch_d_unpermute4(n, inv, lx[last_x], sx[last_x], num_sms, stream);
         break;
     case PBF_BUF_RHO:
-        launch_l_unpermute1(n, inv, lrho, rho, num_sms, stream);
+        launch_d_unpermute1(n, inv, lrho, rho, num_sms, stream);
         break;
     case PBF_BUF_OMEGA:
-        launch_l_unpermute4(n, inv, lom, somega, num_sms, stream);
+        launch_d_unpermute4(n, inv, lom, somega, num_sms, stream);
         break;
     case PBF_BUF_VPRED:
-        launch_l_unpermute4(n, inv, lv, sv, num_sms, stream);
+        launch_d_unpermute4(n, inv, lv, sv, num_sms, stream);
         break;
     default:
         return PBF_OK;
@@ -580,43 +544,6 @@ int pbf_handle::stage(int st, uint32_t iter)
     const DevParams P = dev_params();
     const int sms = num_sms;
     const int mode = effective_mode();
-    if (mode == 6) {
-        switch (st) {
-        case PBF_STAGE_LAMBDA: {
-            prof_begin(PBF_STAGE_LAMBDA);
-            if (iter <= 1)
-                launch_l_lambda_build(P, table, sx[0], order, inv, lxb, lx[1], lrho, list, lcnt, list_cap,
-                                      (1.0f + list_skin) * derived.h, stream);
-            else
-                launch_l_lambda(P, list_args(), lx[0], lx[1], lrho, stream);
-            ++launches;
-            last_x = 1;
-            prof_end(PBF_STAGE_LAMBDA);
-            return PBF_OK;
-        }
-        case PBF_STAGE_DELTAP:
-            prof_begin(PBF_STAGE_DELTAP);
-            launch_l_deltap(P, list_args(), lx[1], lx[0], stream);
-            ++launches;
-            last_x = 0;
-            prof_end(PBF_STAGE_DELTAP);
-            return PBF_OK;
-        case PBF_STAGE_INTEGRATE:
-            prof_begin(PBF_STAGE_INTEGRATE);
-            launch_l_integrate(P, list_args(), lx[0], lv, lx0, lom, lid, pos, vel, stream);
-            ++launches;
-            prof_end(PBF_STAGE_INTEGRATE);
-            return PBF_OK;
-        case PBF_STAGE_VORTICITY:
-            prof_begin(PBF_STAGE_VORTICITY);
-            launch_l_vorticity(P, list_args(), lx0, lom, lid, vel, stream);
-            ++launches;
-            prof_end(PBF_STAGE_VORTICITY);
-            return PBF_OK;
-        default:
-            break;  // predict, sort, table, reorder: below
-        }
-    }
     if (mode == 8 && st >= PBF_STAGE_LAMBDA && st <= PBF_STAGE_VORTICITY) {
         if (!label_space || !dwin_ready) return set_error(PBF_ERR_INVALID, "mode 8: run the reorder stage first");
         DenseArgs D = dense_args();
@@ -741,94 +668,39 @@ int pbf_handle::stage(int st, uint32_t iter)
             prof_end(PBF_STAGE_REORDER);
             break;
         }
-        launch_reorder(P, ids, pos, vel, sx[0], sv, sx0, lod, mode ? mcode : nullptr, sms, stream);
+        launch_reorder(P, ids, pos, vel, sx[0], sv, sx0, lod, mcode, sms, stream);
         ++launches;
-        if (mode) {
+        {
             uint32_t* msorted = nullptr;
             launch_radix_sort(n, 24, mcode, mka, mia, mkb, mib, hist, totals, &msorted, &order, stream, &launches);
-            if (mode == 2) launch_cell_runs(n, msorted, run_blocks, scalars + 2, run_starts, stream, &launches);
         }
         label_space = false;
-        if (mode == 6) {
-            int rc = ensure_list_capacity();
-            if (rc) return rc;
-            launch_l_permute(n, order, ids, skeys, sx[0], sv, sx0, lx[0], lxb, lv, lx0, lid, lkey, inv, sms, stream);
-            ++launches;
-            CK(cudaMemsetAsync(fastb, 0, derived.hash_size, stream));
-            CK(cudaMemsetAsync(lstats, 0, sizeof(uint32_t) * 4, stream));
-            label_space = true;
-        }
         last_x = 0;
         prof_end(PBF_STAGE_REORDER);
         break;
     case PBF_STAGE_LAMBDA:
         prof_begin(PBF_STAGE_LAMBDA);
-        if (mode == 2)
-            launch_lambda_coop(P, sx[0], sx[1], rho, table, lod, iter, order, run_starts, scalars + 2, sms, stream);
-        else if (mode == 3)
-            launch_lambda_q(P, sx[0], sx[1], rho, table, lod, iter, order, stream);
-        else if (mode == 4)
-            launch_lambda_m(P, sx[0], sx[1], rho, table, lod, iter, order, stream);
-        else if (mode == 5)
-            launch_lambda_s(P, sx[0], sx[1], rho, table, lod, iter, order, device, stream);
-        else if (mode == 7)
-            launch_lambda_b(P, sx[0], sx[1], rho, table, lod, iter, order, mcode, scalars + 3, stream);
-        else
-            launch_lambda(P, sx[0], sx[1], rho, table, lod, iter, order, stream);
+        launch_lambda_m(P, sx[0], sx[1], rho, table, lod, iter, order, stream);
         ++launches;
         last_x = 1;
         prof_end(PBF_STAGE_LAMBDA);
         break;
     case PBF_STAGE_DELTAP:
         prof_begin(PBF_STAGE_DELTAP);
-        if (mode == 2)
-            launch_deltap_coop(P, sx[1], sx[0], table, lod, iter, order, run_starts, scalars + 2, sms, stream);
-        else if (mode == 3)
-            launch_deltap_q(P, sx[1], sx[0], table, lod, iter, order, stream);
-        else if (mode == 4)
-            launch_deltap_m(P, sx[1], sx[0], table, lod, iter, order, stream);
-        else if (mode == 5)
-            launch_deltap_s(P, sx[1], sx[0], table, lod, iter, order, device, stream);
-        else if (mode == 7)
-            launch_deltap_b(P, sx[1], sx[0], table, lod, iter, order, mcode, scalars + 3, stream);
-        else
-            launch_deltap_apply(P, sx[1], sx[0], table, lod, iter, order, stream);
+        launch_deltap_m(P, sx[1], sx[0], table, lod, iter, order, stream);
         ++launches;
         last_x = 0;
         prof_end(PBF_STAGE_DELTAP);
         break;
     case PBF_STAGE_INTEGRATE:
         prof_begin(PBF_STAGE_INTEGRATE);
-        if (mode == 2)
-            launch_integrate_coop(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, run_starts, scalars + 2,
-                                  sms, stream);
-        else if (mode == 3)
-            launch_integrate_q(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, stream);
-        else if (mode == 4)
-            launch_integrate_m(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, stream);
-        else if (mode == 5)
-            launch_integrate_s(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, device, stream);
-        else if (mode == 7)
-            launch_integrate_b(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, mcode, scalars + 3, stream);
-        else
-            launch_integrate(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, stream);
+        launch_integrate_m(P, sx[0], sv, sx0, somega, ids, pos, vel, table, order, stream);
         ++launches;
         prof_end(PBF_STAGE_INTEGRATE);
         break;
     case PBF_STAGE_VORTICITY:
         prof_begin(PBF_STAGE_VORTICITY);
-        if (mode == 2)
-            launch_vorticity_coop(P, sx0, somega, ids, vel, table, order, run_starts, scalars + 2, sms, stream);
-        else if (mode == 3)
-            launch_vorticity_q(P, sx0, somega, ids, vel, table, order, stream);
-        else if (mode == 4)
-            launch_vorticity_m(P, sx0, somega, ids, vel, table, order, stream);
-        else if (mode == 5)
-            launch_vorticity_s(P, sx0, somega, ids, vel, table, order, device, stream);
-        else if (mode == 7)
-            launch_vorticity_b(P, sx0, somega, ids, vel, table, order, mcode, scalars + 3, stream);
-        else
-            launch_vorticity(P, sx0, somega, ids, vel, table, order, stream);
+        launch_vorticity_m(P, sx0, somega, ids, vel, table, order, stream);
         ++launches;
         prof_end(PBF_STAGE_VORTICITY);
         break;
@@ -857,10 +729,6 @@ int pbf_handle::step_body()
 int pbf_handle::step()
 {
     if (n == 0) return PBF_OK;  // PBFluids.cpp:325
-    if (effective_mode() == 6) {
-        const int rc = ensure_list_capacity();  // before any capture
-        if (rc) return rc;
-    }
     if (effective_mode() == 8) {
         const int rc = ensure_dense();  // allocation and slot flags before any capture
         if (rc) return rc;
@@ -921,8 +789,6 @@ extern "C" int pbf_create(const pbf_fluid_config* cfg, int device, pbf_handle** 
     h->cfg = *cfg;
     for (int i = 0; i < PBF_NUM_PASS_SLOTS; ++i) h->prof_open[i] = -1;
     cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
-    staged_init(device);
-    brick_init(device);
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         delete h;
@@ -1414,13 +1280,10 @@ extern "C" int pbf_set_option(pbf_handle* h, int option, int value)
     if (!h) return set_error(PBF_ERR_INVALID, "null handle");
     switch (option) {
     case PBF_OPT_SPATIAL_ORDER:
-        if (value < -1 || value > 8) return set_error(PBF_ERR_INVALID, "spatial order mode %d", value);
+        if (value != -1 && value != 4 && value != 8)
+            return set_error(PBF_ERR_INVALID, "neighbour mode %d: -1 (automatic), 4 or 8", value);
         h->pass_mode = value;
         h->label_space = false;
-        break;
-    case PBF_OPT_LIST_SKIN:
-        if (value < 1 || value > 1000) return set_error(PBF_ERR_INVALID, "list skin %d not in [1, 1000] (1/1000 h)", value);
-        h->list_skin = (float)value * 1e-3f;
         break;
     default: return set_error(PBF_ERR_INVALID, "unknown option %d", option);
     }
@@ -1446,27 +1309,7 @@ extern "C" int pbf_list_stats(pbf_handle* h, uint32_t* full_walks, uint32_t* buc
             *bucket_walks = d3[0];
             *marked_buckets = d3[2];
         }
-        return PBF_OK;
     }
-    if (h->effective_mode() == 7) {
-        // mode 7: blocks that walked global memory instead of their staged
-        // neighbourhood, counted since the handle was created
-        if (h->scalars) {
-            uint32_t d2[2];
-            CK(cudaMemcpyAsync(d2, h->scalars + 3, sizeof(d2), cudaMemcpyDeviceToHost, h->stream));
-            CK(cudaStreamSynchronize(h->stream));
-            *full_walks = d2[0];    // blocks
-            *bucket_walks = d2[1];  // particles
-        }
-        return PBF_OK;
-    }
-    if (!h->lstats) return PBF_OK;
-    uint32_t d[4];
-    CK(cudaMemcpyAsync(d, h->lstats, sizeof(d), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    *full_walks = d[0];
-    *bucket_walks = d[1];
-    *marked_buckets = d[2];
     return PBF_OK;
 }
 

@@ -40,30 +40,20 @@ struct pbf_handle {
     uint32_t* totals = nullptr;
     int2* table = nullptr;
     // spatial processing order of the neighbour passes (Morton order of the
-    // predict-time cells); `order` points into one of the m* ping-pong pairs
-    // PBF_OPT_SPATIAL_ORDER: 0 hash order, 1 Morton order, 2 Morton cell-cooperative,
-    // 3 Morton + per-lane pair queues, 4 Morton + per-bucket hit masks, 5-7 staged /
-    // listed variants, 8 x-runs of the dense cell window; -1 (default): 8 from
-    // 2^19 particles, 4 below
+    // predict-time cells); `order` points into one of the m* ping-pong pairs.
+    // PBF_OPT_SPATIAL_ORDER: 4 hashed buckets in Morton thread order with
+    // per-bucket hit masks, 8 x-runs of the dense cell window; -1 (default): 8
+    // from 2^19 particles, 4 below
     int pass_mode = -1;
     uint32_t *mcode = nullptr, *mka = nullptr, *mia = nullptr, *mkb = nullptr, *mib = nullptr;
     uint32_t* order = nullptr;
-    // cell runs of the Morton order (one warp per run in the cooperative passes)
-    uint32_t* run_starts = nullptr;
-    uint32_t* run_blocks = nullptr;
-    // mode 6: neighbour lists over Morton-labelled copies of the sorted arrays
+    // mode 8: the per-particle arrays relabelled by window slot
     float4 *lx[2] = {nullptr, nullptr}, *lxb = nullptr, *lv = nullptr, *lx0 = nullptr, *lom = nullptr;
     float* lrho = nullptr;
-    uint32_t *lid = nullptr, *lkey = nullptr, *inv = nullptr, *list = nullptr, *lcnt = nullptr;
-    uint32_t* lstats = nullptr;  // 4 counters of the last substep
-    uint8_t* fastb = nullptr;    // per bucket (hash size)
-    uint32_t cap_fast = 0;
-    uint32_t cap_list_n = 0;
-    uint32_t list_cap = 64;      // entries per particle
-    float list_skin = 0.1f;      // in units of h
+    uint32_t *lid = nullptr, *lkey = nullptr, *inv = nullptr;
     bool label_space = false;    // the current substep's state lives in the label arrays
     uint32_t cap_label_n = 0;
-    // mode 8: runs of a dense cell window (label arrays shared with mode 6)
+    // mode 8: runs of a dense cell window
     int2* dtable = nullptr;      // per window slot: label range
     int2* druns = nullptr;       // per window slot: label range of its x-run (slots s-1 .. s+1)
     uint8_t* dclean = nullptr;   // per window slot: no hash collision near the cell
@@ -92,8 +82,6 @@ struct pbf_handle {
     pbf::DenseArgs dense_args() const;
     int effective_mode() const;
     int ensure_label_capacity();
-    int ensure_list_capacity();
-    pbf::ListArgs list_args() const;
     int unpermute_for_read(int which);
     // sorted order
     float4* sx[2] = {nullptr, nullptr};

@@ -14,51 +14,12 @@ void launch_predict_hash(const DevParams& P, const float4* pos, const float4* ve
 void launch_reorder(const DevParams& P, const uint32_t* ids, const float4* pos, const float4* vel, float4* sx,
                     float4* sv, float4* sx0, uint32_t* lod, uint32_t* mcode, int sms, cudaStream_t st);
 void launch_build_table(uint32_t n, const uint32_t* sk, int2* table, int sms, cudaStream_t st);
-void launch_lambda(const DevParams& P, const float4* xin, float4* xout, float* rho, const int2* table,
-                   const uint32_t* lod, uint32_t iter, const uint32_t* order, cudaStream_t st);
-void launch_deltap_apply(const DevParams& P, const float4* xin, float4* xout, const int2* table,
-                         const uint32_t* lod, uint32_t iter, const uint32_t* order, cudaStream_t st);
-void launch_integrate(const DevParams& P, const float4* xs, const float4* sv, float4* sx0, float4* somega,
-                      const uint32_t* ids, float4* pos, float4* vel, const int2* table, const uint32_t* order,
-                      cudaStream_t st);
-void launch_vorticity(const DevParams& P, const float4* spos, const float4* somega, const uint32_t* ids,
-                      float4* vel, const int2* table, const uint32_t* order, cudaStream_t st);
 void launch_check_finite(uint32_t n, const float4* pos, const float4* vel, uint32_t* bad, int sms,
                          cudaStream_t st);
 void launch_unpack_particles(uint32_t n, const float4* aos, float4* pos, float4* pred, float4* vel, int sms,
                              cudaStream_t st);
 void launch_pack_particles(uint32_t n, const float4* pos, const float4* pred, const float4* vel, float4* aos,
                            int sms, cudaStream_t st);
-
-// ---- k_coop.cu: cell-cooperative neighbour passes ----------------------------
-// Runs of equal codes in the sorted Morton list (the cells); run_starts gets
-// run_count + 1 entries (last = n).  Scratch: head_num_blocks(n) counts.
-uint32_t head_num_blocks(uint32_t n);
-void launch_cell_runs(uint32_t n, const uint32_t* sorted_codes, uint32_t* block_counts, uint32_t* run_count,
-                      uint32_t* run_starts, cudaStream_t st, uint64_t* launches);
-void launch_lambda_coop(const DevParams& P, const float4* xin, float4* xout, float* rho, const int2* table,
-                        const uint32_t* lod, uint32_t iter, const uint32_t* order, const uint32_t* runs,
-                        const uint32_t* run_count, int sms, cudaStream_t st);
-void launch_deltap_coop(const DevParams& P, const float4* xin, float4* xout, const int2* table, const uint32_t* lod,
-                        uint32_t iter, const uint32_t* order, const uint32_t* runs, const uint32_t* run_count, int sms,
-                        cudaStream_t st);
-void launch_integrate_coop(const DevParams& P, const float4* xs, const float4* sv, float4* sx0, float4* somega,
-                           const uint32_t* ids, float4* pos, float4* vel, const int2* table, const uint32_t* order,
-                           const uint32_t* runs, const uint32_t* run_count, int sms, cudaStream_t st);
-void launch_vorticity_coop(const DevParams& P, const float4* spos, const float4* somega, const uint32_t* ids,
-                           float4* vel, const int2* table, const uint32_t* order, const uint32_t* runs,
-                           const uint32_t* run_count, int sms, cudaStream_t st);
-
-// ---- k_queue.cu: thread per particle, in-range pairs queued per lane ---------
-void launch_lambda_q(const DevParams& P, const float4* xin, float4* xout, float* rho, const int2* table,
-                     const uint32_t* lod, uint32_t iter, const uint32_t* order, cudaStream_t st);
-void launch_deltap_q(const DevParams& P, const float4* xin, float4* xout, const int2* table, const uint32_t* lod,
-                     uint32_t iter, const uint32_t* order, cudaStream_t st);
-void launch_integrate_q(const DevParams& P, const float4* xs, const float4* sv, float4* sx0, float4* somega,
-                        const uint32_t* ids, float4* pos, float4* vel, const int2* table, const uint32_t* order,
-                        cudaStream_t st);
-void launch_vorticity_q(const DevParams& P, const float4* spos, const float4* somega, const uint32_t* ids,
-                        float4* vel, const int2* table, const uint32_t* order, cudaStream_t st);
 
 // ---- k_masked.cu: thread per particle, bucket chunks tested into a hit mask --
 void launch_lambda_m(const DevParams& P, const float4* xin, float4* xout, float* rho, const int2* table,
@@ -70,62 +31,6 @@ void launch_integrate_m(const DevParams& P, const float4* xs, const float4* sv, 
                         cudaStream_t st);
 void launch_vorticity_m(const DevParams& P, const float4* spos, const float4* somega, const uint32_t* ids,
                         float4* vel, const int2* table, const uint32_t* order, cudaStream_t st);
-
-// ---- k_staged.cu: 256-particle cell blocks staged through shared memory -------
-void staged_init(int device);  // opt the kernels into > 48 KB of shared memory
-void launch_lambda_s(const DevParams& P, const float4* xin, float4* xout, float* rho, const int2* table,
-                     const uint32_t* lod, uint32_t iter, const uint32_t* order, int device, cudaStream_t st);
-void launch_deltap_s(const DevParams& P, const float4* xin, float4* xout, const int2* table, const uint32_t* lod,
-                     uint32_t iter, const uint32_t* order, int device, cudaStream_t st);
-void launch_integrate_s(const DevParams& P, const float4* xs, const float4* sv, float4* sx0, float4* somega,
-                        const uint32_t* ids, float4* pos, float4* vel, const int2* table, const uint32_t* order,
-                        int device, cudaStream_t st);
-void launch_vorticity_s(const DevParams& P, const float4* spos, const float4* somega, const uint32_t* ids,
-                        float4* vel, const int2* table, const uint32_t* order, int device, cudaStream_t st);
-
-// ---- k_brick.cu: per-block neighbourhood staged in shared memory (dense cells) --
-// mcode: the reorder kernel's Morton code of each slot's predict-time cell;
-// stats (may be null): [0] blocks, [1] particles that walked global memory.
-void brick_init(int device);
-void launch_lambda_b(const DevParams& P, const float4* xin, float4* xout, float* rho, const int2* table,
-                     const uint32_t* lod, uint32_t iter, const uint32_t* order, const uint32_t* mcode,
-                     uint32_t* stats, cudaStream_t st);
-void launch_deltap_b(const DevParams& P, const float4* xin, float4* xout, const int2* table, const uint32_t* lod,
-                     uint32_t iter, const uint32_t* order, const uint32_t* mcode, uint32_t* stats, cudaStream_t st);
-void launch_integrate_b(const DevParams& P, const float4* xs, const float4* sv, float4* sx0, float4* somega,
-                        const uint32_t* ids, float4* pos, float4* vel, const int2* table, const uint32_t* order,
-                        const uint32_t* mcode, uint32_t* stats, cudaStream_t st);
-void launch_vorticity_b(const DevParams& P, const float4* spos, const float4* somega, const uint32_t* ids,
-                        float4* vel, const int2* table, const uint32_t* order, const uint32_t* mcode,
-                        uint32_t* stats, cudaStream_t st);
-
-// ---- k_list.cu: neighbour lists with a skin over Morton-labelled data ----------
-struct ListArgs {
-    const int2* table;
-    const uint32_t* inv;   // hash slot -> label
-    const uint32_t* list;  // cap x n, column-major: bucket index << 27 | label
-    const uint32_t* cnt;   // entries per label (0xFFFFFFFF = overflowed)
-    const float4* xb;      // build positions, label order
-    const uint32_t* lkey;  // bucket (predict-time hash) of each label
-    uint8_t* fastb;        // per bucket: holds a particle that moved > skin/2
-    uint32_t* stats;       // [0] full walks, [1] marked-bucket walks, [2] marked buckets
-    float half_skin2;      // (skin/2 - rounding margin)^2
-};
-void launch_l_permute(uint32_t n, const uint32_t* order, const uint32_t* ids, const uint32_t* skeys,
-                      const float4* sx, const float4* sv, const float4* sx0, float4* lx, float4* lxb, float4* lv,
-                      float4* lx0, uint32_t* lid, uint32_t* lkey, uint32_t* inv, int sms, cudaStream_t st);
-void launch_l_lambda_build(const DevParams& P, const int2* table, const float4* sx, const uint32_t* order,
-                           const uint32_t* inv, const float4* lxb, float4* lx_out, float* lrho, uint32_t* list,
-                           uint32_t* cnt, uint32_t cap, float reach, cudaStream_t st);
-void launch_l_lambda(const DevParams& P, const ListArgs& A, const float4* lx_in, float4* lx_out, float* lrho,
-                     cudaStream_t st);
-void launch_l_deltap(const DevParams& P, const ListArgs& A, const float4* lx_in, float4* lx_out, cudaStream_t st);
-void launch_l_integrate(const DevParams& P, const ListArgs& A, const float4* lx, const float4* lv, float4* lx0,
-                        float4* lom, const uint32_t* lid, float4* pos, float4* vel, cudaStream_t st);
-void launch_l_vorticity(const DevParams& P, const ListArgs& A, const float4* lx0, const float4* lom,
-                        const uint32_t* lid, float4* vel, cudaStream_t st);
-void launch_l_unpermute4(uint32_t n, const uint32_t* inv, const float4* src, float4* dst, int sms, cudaStream_t st);
-void launch_l_unpermute1(uint32_t n, const uint32_t* inv, const float* src, float* dst, int sms, cudaStream_t st);
 
 // ---- k_dense.cu: x-runs of a dense cell window over relabelled data ----------
 constexpr int kDenseListWords = 16;
@@ -193,6 +98,8 @@ void launch_d_integrate(const DevParams& P, const DenseArgs& D, const float4* lx
                         float4* lom, const uint32_t* lid, float4* pos, float4* vel, cudaStream_t st);
 void launch_d_vorticity(const DevParams& P, const DenseArgs& D, const float4* lx0, const float4* lom,
                         const uint32_t* lid, float4* vel, cudaStream_t st);
+void launch_d_unpermute4(uint32_t n, const uint32_t* inv, const float4* src, float4* dst, int sms, cudaStream_t st);
+void launch_d_unpermute1(uint32_t n, const uint32_t* inv, const float* src, float* dst, int sms, cudaStream_t st);
 
 // ---- k_sort.cu ----------------------------------------------------------------
 // Keys per sort tile: one 256-digit histogram per tile, so scratch sized for

@@ -366,10 +366,9 @@ class PBFluids:
         check(lib().pbf_set_option(self._h, int(option), int(value)))
 
     def list_stats(self):
-        """Mode 6, last substep, summed over passes: (particles that walked
-        all buckets, marked buckets walked in full, buckets marked).  Mode 8:
-        (particle passes that walked the hashed buckets, drift bound exceeded
-        in the last substep, window cells with a hash collision nearby)."""
+        """Mode 8: (particle passes that walked the hashed buckets, drift bound
+        exceeded in the last substep, window cells with a hash collision
+        nearby); zeros in mode 4."""
         a, b, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
         check(lib().pbf_list_stats(self._h, C.byref(a), C.byref(b), C.byref(c)))
         return a.value, b.value, c.value
