@@ -4,6 +4,7 @@ TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
 CPU-baseline legs of bench.py, never by the product path.
 
   liboracle.so         FP64 restatement (oracle/pbf_oracle.c, sdf_oracle.c)
+  liboracle32.so       the same sources with float32 storage (orc_real = float)
   _ref/libpbfref_cpu.so   reference src/fluid/Kernels.cpp + NeighborSearch.cpp
   _ref/libpbfref_glsl.so  reference compute shaders run on the CPU
   _ref/libpbfref_sdf.so   reference src/fluid/SDFBoundary.cpp (mesh SDF, BVH)
@@ -17,6 +18,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+LIB32_PATH = os.path.join(HERE, "_build", "liboracle32.so")
 REF_CPU_PATH = os.path.join(HERE, "_ref", "libpbfref_cpu.so")
 REF_GLSL_PATH = os.path.join(HERE, "_ref", "libpbfref_glsl.so")
 REF_SDF_PATH = os.path.join(HERE, "_ref", "libpbfref_sdf.so")
@@ -294,6 +296,87 @@ def adjoint_step(params, pos0, vel0, gpos=None, gvel=None, sdf=None):
     lib().orc_adjoint_step(C.byref(params.p), sdf.ref() if sdf else None, n, p0, v0, _ptr(gp), _ptr(gv), gp0, gv0,
                            gt, _ptr(pT), _ptr(vT))
     return gp0.reshape(n, 3), gv0.reshape(n, 3), gt, pT.reshape(n, 3), vT.reshape(n, 3)
+
+
+# ---- float32 build of the same restatement ------------------------------------
+def _f32_fields(fields):
+    return [(n, (C.c_float * t._length_) if (hasattr(t, "_length_") and t._type_ is C.c_double)
+             else (C.c_float if t is C.c_double else t)) for n, t in fields]
+
+
+class OrcParams32(C.Structure):
+    _fields_ = _f32_fields(OrcParams._fields_)
+
+
+class OrcSdf32(C.Structure):
+    _fields_ = _f32_fields(OrcSdf._fields_)
+
+
+_lib32 = None
+
+
+def lib32():
+    """liboracle32.so: the restatement with float32 storage and sequential
+    sums (oracle/pbf_oracle.h, orc_real)."""
+    global _lib32
+    if _lib32 is None:
+        if not os.path.exists(LIB32_PATH):
+            build()
+        L = C.CDLL(LIB32_PATH)
+        L.orc_derive.argtypes = [C.POINTER(FluidConfig), C.c_float, C.POINTER(OrcParams32)]
+        L.orc_step.argtypes = [C.POINTER(OrcParams32), C.c_void_p, C.c_uint32, f32p, f32p, C.c_void_p, C.c_void_p,
+                               C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_adjoint_step.argtypes = [C.POINTER(OrcParams32), C.c_void_p, C.c_uint32, f32p, f32p, C.c_void_p,
+                                       C.c_void_p, f32p, f32p, f32p, C.c_void_p, C.c_void_p]
+        _lib32 = L
+    return _lib32
+
+
+class Params32:
+    """Derived parameters of a FluidConfig for the float32 build."""
+
+    def __init__(self, cfg):
+        self.p = OrcParams32()
+        lib32().orc_derive(C.byref(cfg), 0.0, C.byref(self.p))
+        self.cfg = cfg
+
+
+class Sdf32:
+    def __init__(self, dist, origin, cell, padding=0.0, containment=False):
+        self.dist = np.ascontiguousarray(dist, dtype=np.float32)
+        self.s = OrcSdf32()
+        self.s.enabled = 1
+        self.s.dims[:] = list(self.dist.shape)
+        self.s.origin[:] = [float(v) for v in origin]
+        self.s.cell = float(cell)
+        self.s.dist = self.dist.ctypes.data_as(C.POINTER(C.c_float))
+        self.s.padding = float(padding)
+        self.s.containment = 1 if containment else 0
+
+    def ref(self):
+        return C.byref(self.s)
+
+
+def step32(params, pos, vel, sdf=None):
+    """One step of the float32 build; pos/vel (n,3) float32, updated in place."""
+    assert pos.dtype == np.float32 and vel.dtype == np.float32
+    lib32().orc_step(C.byref(params.p), sdf.ref() if sdf else None, len(pos), pos.reshape(-1), vel.reshape(-1),
+                     None, None, None, None, None)
+
+
+def adjoint_step32(params, pos0, vel0, gpos=None, gvel=None, sdf=None):
+    """adjoint_step in the float32 build: (gpos0, gvel0, gt) as float32."""
+    n = len(pos0)
+    p0 = np.ascontiguousarray(pos0, dtype=np.float32).reshape(-1)
+    v0 = np.ascontiguousarray(vel0, dtype=np.float32).reshape(-1)
+    gp = None if gpos is None else np.ascontiguousarray(gpos, dtype=np.float32).reshape(-1)
+    gv = None if gvel is None else np.ascontiguousarray(gvel, dtype=np.float32).reshape(-1)
+    gp0 = np.zeros(3 * n, np.float32)
+    gv0 = np.zeros(3 * n, np.float32)
+    gt = np.zeros(3, np.float32)
+    lib32().orc_adjoint_step(C.byref(params.p), sdf.ref() if sdf else None, n, p0, v0, _ptr(gp), _ptr(gv), gp0, gv0,
+                             gt, None, None)
+    return gp0.reshape(n, 3), gv0.reshape(n, 3), gt
 
 
 # ---- reference builds -------------------------------------------------------

@@ -1,7 +1,7 @@
 /*
  * pbf_oracle.c — FP64 CPU restatement of the reference PBF substep.
  *
- * TEST INFRASTRUCTURE ONLY (see pbf_oracle.h).  Restates, in double
+ * TEST INFRASTRUCTURE ONLY (see pbf_oracle.h).  Restates, in orc_real
  * precision, the math of the reference compute shaders under
  * resources/shaders/compute/ and of PBFluids::setParams/step
  * (src/fluid/PBFluids.cpp).  OpenMP-parallel over particles so that it also
@@ -17,22 +17,22 @@
 #define M_PI 3.14159265358979323846
 #endif
 
-static inline double clampd(double v, double lo, double hi) { return v < lo ? lo : (v > hi ? hi : v); }
-static inline double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+static inline orc_real clampd(orc_real v, orc_real lo, orc_real hi) { return v < lo ? lo : (v > hi ? hi : v); }
+static inline orc_real dot3(const orc_real* a, const orc_real* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 
 /* PBFluids::setParams + setBounds (src/fluid/PBFluids.cpp:39-109, 299-306). */
-void orc_derive(const pbf_fluid_config* c, double pad, orc_params* p)
+void orc_derive(const pbf_fluid_config* c, orc_real pad, orc_params* p)
 {
     memset(p, 0, sizeof(*p));
     for (int a = 0; a < 3; ++a) {
-        p->bmin[a] = (double)c->bounds_min[a] + pad; /* PBFluids.cpp:303 */
-        p->bmax[a] = (double)c->bounds_max[a] - pad; /* PBFluids.cpp:304 */
+        p->bmin[a] = (orc_real)c->bounds_min[a] + pad; /* PBFluids.cpp:303 */
+        p->bmax[a] = (orc_real)c->bounds_max[a] - pad; /* PBFluids.cpp:304 */
         p->g[a] = c->gravity[a];
     }
     p->damping = clampd(c->bound_damping, 0.0, 1.0); /* PBFluids.cpp:305 */
     p->substeps = c->substep_iterations;
-    p->dt = (double)c->dt / (double)c->substep_iterations; /* PBFluids.cpp:52 */
-    const double h = c->h;
+    p->dt = (orc_real)c->dt / (orc_real)c->substep_iterations; /* PBFluids.cpp:52 */
+    const orc_real h = c->h;
     p->h = h;
     p->h2 = h * h;
     p->rho0 = c->rho0;
@@ -40,8 +40,8 @@ void orc_derive(const pbf_fluid_config* c, double pad, orc_params* p)
     /* wq = calcSCorrKernel((dq,0,0), h) = poly6 at dq (PBFluids.cpp:45-46,
      * Kernels.cpp:9-27,216-219) */
     {
-        const double dq = (double)c->delta_q * h;
-        const double r2 = dq * dq;
+        const orc_real dq = (orc_real)c->delta_q * h;
+        const orc_real r2 = dq * dq;
         p->wq = (r2 > p->h2) ? 0.0 : (315.0 / (64.0 * M_PI)) / pow(h, 9.0) * pow(p->h2 - r2, 3.0);
     }
     p->k_corr = c->k_corr;
@@ -53,7 +53,7 @@ void orc_derive(const pbf_fluid_config* c, double pad, orc_params* p)
     p->w0_self = (315.0 / (64.0 * M_PI)) / (h * h * h); /* PBFluids.cpp:83 */
     p->poly6 = 315.0 / (64.0 * M_PI * pow(h, 9.0));     /* PBFluids.cpp:86 */
     p->spiky = 45.0 / (M_PI * pow(h, 6.0));             /* PBFluids.cpp:89 */
-    p->inv_rho0 = 1.0 / (double)c->rho0;                /* PBFluids.cpp:92 */
+    p->inv_rho0 = 1.0 / (orc_real)c->rho0;                /* PBFluids.cpp:92 */
     p->hash_size = c->hash_size;
     p->mask = c->hash_size - 1u; /* PBFluids.cpp:95 */
     p->scorr = c->enable_scorr ? 1u : 0u;
@@ -74,7 +74,7 @@ uint32_t orc_hash(int32_t cx, int32_t cy, int32_t cz, uint32_t mask)
     return n & mask;
 }
 
-static inline void cell_of(const double* x, double h, int32_t c[3])
+static inline void cell_of(const orc_real* x, orc_real h, int32_t c[3])
 {
     for (int a = 0; a < 3; ++a) c[a] = (int32_t)floor(x[a] / h);
 }
@@ -121,45 +121,45 @@ void orc_build_table(const uint32_t* sk, uint32_t n, uint32_t hash_size, int32_t
 }
 
 /* ---- SDF grid sampling ---------------------------------------------------- */
-static inline double texel(const orc_sdf* s, int x, int y, int z)
+static inline orc_real texel(const orc_sdf* s, int x, int y, int z)
 {
     x = x < 0 ? 0 : (x >= s->dims[0] ? s->dims[0] - 1 : x);
     y = y < 0 ? 0 : (y >= s->dims[1] ? s->dims[1] - 1 : y);
     z = z < 0 ? 0 : (z >= s->dims[2] ? s->dims[2] - 1 : z);
-    return (double)s->dist[((int64_t)x * s->dims[1] + y) * s->dims[2] + z];
+    return (orc_real)s->dist[((int64_t)x * s->dims[1] + y) * s->dims[2] + z];
 }
 
 /* texture(sdfTexture, ((p - o)/cell + 0.5)/dims) with GL_LINEAR and
  * CLAMP_TO_EDGE (CS_Integrate.glsl:86-89, src/opengl/Texture3D.cpp:25-32):
  * texel-space coordinate u = (p - o)/cell, texel i centred on integer i. */
-double orc_sdf_query(const orc_sdf* s, const double p[3])
+orc_real orc_sdf_query(const orc_sdf* s, const orc_real p[3])
 {
-    double u[3];
+    orc_real u[3];
     int i0[3];
-    double a[3];
+    orc_real a[3];
     for (int k = 0; k < 3; ++k) {
-        u[k] = clampd((p[k] - s->origin[k]) / s->cell, 0.0, (double)(s->dims[k] - 1));
+        u[k] = clampd((p[k] - s->origin[k]) / s->cell, 0.0, (orc_real)(s->dims[k] - 1));
         i0[k] = (int)floor(u[k]);
         a[k] = u[k] - i0[k];
     }
-    double c[2][2][2];
+    orc_real c[2][2][2];
     for (int dx = 0; dx < 2; ++dx)
         for (int dy = 0; dy < 2; ++dy)
             for (int dz = 0; dz < 2; ++dz) c[dx][dy][dz] = texel(s, i0[0] + dx, i0[1] + dy, i0[2] + dz);
-    double cz[2][2];
+    orc_real cz[2][2];
     for (int dx = 0; dx < 2; ++dx)
         for (int dy = 0; dy < 2; ++dy) cz[dx][dy] = c[dx][dy][0] + (c[dx][dy][1] - c[dx][dy][0]) * a[2];
-    double cy[2];
+    orc_real cy[2];
     for (int dx = 0; dx < 2; ++dx) cy[dx] = cz[dx][0] + (cz[dx][1] - cz[dx][0]) * a[1];
     return cy[0] + (cy[1] - cy[0]) * a[0];
 }
 
 /* sdfGradient: central differences with e = cell (CS_Integrate.glsl:92-99) */
-void orc_sdf_gradient(const orc_sdf* s, const double p[3], double g[3])
+void orc_sdf_gradient(const orc_sdf* s, const orc_real p[3], orc_real g[3])
 {
-    const double e = s->cell;
+    const orc_real e = s->cell;
     for (int k = 0; k < 3; ++k) {
-        double pp[3] = {p[0], p[1], p[2]}, pm[3] = {p[0], p[1], p[2]};
+        orc_real pp[3] = {p[0], p[1], p[2]}, pm[3] = {p[0], p[1], p[2]};
         pp[k] += e;
         pm[k] -= e;
         g[k] = (orc_sdf_query(s, pp) - orc_sdf_query(s, pm)) / (2.0 * e);
@@ -167,56 +167,56 @@ void orc_sdf_gradient(const orc_sdf* s, const double p[3], double g[3])
 }
 
 /* ---- kernels (CS_ComputeLambdas.glsl:74-92) ------------------------------ */
-static inline double poly6(const orc_params* p, double r2)
+static inline orc_real poly6(const orc_params* p, orc_real r2)
 {
     if (r2 > p->h2) return 0.0;
-    const double d = p->h2 - r2;
+    const orc_real d = p->h2 - r2;
     return p->poly6 * d * d * d;
 }
 
-static inline void grad_spiky(const orc_params* p, const double r[3], double r2, double g[3])
+static inline void grad_spiky(const orc_params* p, const orc_real r[3], orc_real r2, orc_real g[3])
 {
     if (r2 > p->h2 || r2 < 1e-10) {
         g[0] = g[1] = g[2] = 0.0;
         return;
     }
-    const double dist = sqrt(r2);
-    const double diff = p->h - dist;
-    const double sc = -p->spiky * diff * diff / dist;
+    const orc_real dist = sqrt(r2);
+    const orc_real diff = p->h - dist;
+    const orc_real sc = -p->spiky * diff * diff / dist;
     g[0] = r[0] * sc;
     g[1] = r[1] * sc;
     g[2] = r[2] * sc;
 }
 
 /* computeSCorr (CS_ComputeDeltaP.glsl:94-104) */
-static inline double scorr(const orc_params* p, double r2)
+static inline orc_real scorr(const orc_params* p, orc_real r2)
 {
     if (!p->scorr) return 0.0;
-    const double w = poly6(p, r2);
+    const orc_real w = poly6(p, r2);
     if (p->wq <= 1e-12 || w <= 0.0) return 0.0;
-    const double ratio = w / p->wq;
+    const orc_real ratio = w / p->wq;
     if (ratio <= 0.0) return 0.0;
     return -p->k_corr * pow(ratio, p->n_corr);
 }
 
 /* ---- passes -------------------------------------------------------------- */
-void orc_predict(const orc_params* p, uint32_t n, const double* pos, double* vel, double* xstar,
+void orc_predict(const orc_params* p, uint32_t n, const orc_real* pos, orc_real* vel, orc_real* xstar,
                  uint32_t* keys)
 {
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < (int64_t)n; ++i) {
-        const double* x = pos + 3 * i;
-        double* v = vel + 3 * i;
+        const orc_real* x = pos + 3 * i;
+        orc_real* v = vel + 3 * i;
         for (int a = 0; a < 3; ++a) v[a] += p->g[a] * p->dt; /* :102 */
         if (p->interacting) {                                 /* :105-112 */
-            double to[3] = {p->i_pos[0] - x[0], p->i_pos[1] - x[1], p->i_pos[2] - x[2]};
-            const double dist = sqrt(dot3(to, to));
+            orc_real to[3] = {p->i_pos[0] - x[0], p->i_pos[1] - x[1], p->i_pos[2] - x[2]};
+            const orc_real dist = sqrt(dot3(to, to));
             if (dist < p->i_radius && dist > 1e-5) {
-                const double falloff = 1.0 - dist / p->i_radius;
+                const orc_real falloff = 1.0 - dist / p->i_radius;
                 for (int a = 0; a < 3; ++a) v[a] += to[a] / dist * p->i_strength * falloff * p->dt;
             }
         }
-        double* xs = xstar + 3 * i;
+        orc_real* xs = xstar + 3 * i;
         for (int a = 0; a < 3; ++a) xs[a] = x[a] + v[a] * p->dt; /* :114 */
         int32_t c[3];
         cell_of(xs, p->h, c); /* :125 */
@@ -224,15 +224,15 @@ void orc_predict(const orc_params* p, uint32_t n, const double* pos, double* vel
     }
 }
 
-void orc_lod(const orc_params* p, uint32_t n, const double* xstar, uint32_t* lod)
+void orc_lod(const orc_params* p, uint32_t n, const orc_real* xstar, uint32_t* lod)
 {
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < (int64_t)n; ++i) {
-        const double* x = xstar + 3 * i;
-        double d[3] = {p->camera[0] - x[0], p->camera[1] - x[1], p->camera[2] - x[2]};
-        const double dist = sqrt(dot3(d, d));
-        const double t = clampd(dist / p->lod_max_dist, 0.0, 1.0);
-        const double m = (double)p->max_lod * (1.0 - t) + (double)p->min_lod * t;
+        const orc_real* x = xstar + 3 * i;
+        orc_real d[3] = {p->camera[0] - x[0], p->camera[1] - x[1], p->camera[2] - x[2]};
+        const orc_real dist = sqrt(dot3(d, d));
+        const orc_real t = clampd(dist / p->lod_max_dist, 0.0, 1.0);
+        const orc_real m = (orc_real)p->max_lod * (1.0 - t) + (orc_real)p->min_lod * t;
         uint32_t l = (uint32_t)rint(m);
         if (l < p->min_lod) l = p->min_lod;
         if (l > p->max_lod) l = p->max_lod;
@@ -260,21 +260,21 @@ void orc_lod(const orc_params* p, uint32_t n, const double* xstar, uint32_t* lod
                 }                                                                            \
     } while (0)
 
-void orc_lambda(const orc_params* p, uint32_t n, const double* xstar, const uint32_t* ids,
-                const int32_t* table, const uint32_t* lod, uint32_t iter, double* lambda, double* rho)
+void orc_lambda(const orc_params* p, uint32_t n, const orc_real* xstar, const uint32_t* ids,
+                const int32_t* table, const uint32_t* lod, uint32_t iter, orc_real* lambda, orc_real* rho)
 {
-    const double ir2 = p->inv_rho0 * p->inv_rho0;
+    const orc_real ir2 = p->inv_rho0 * p->inv_rho0;
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < (int64_t)n; ++i) {
         if (p->apbf && lod && lod[i] < iter) continue; /* :113 */
-        const double* xi = xstar + 3 * i;
-        double rho_i = p->w0_self, sg = 0.0, gi[3] = {0, 0, 0};
+        const orc_real* xi = xstar + 3 * i;
+        orc_real rho_i = p->w0_self, sg = 0.0, gi[3] = {0, 0, 0};
         FOR_EACH_NEIGHBOUR(p, xi, i, ids, table, {
-            const double* xj = xstar + 3 * j;
-            const double r[3] = {xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]};
-            const double r2 = dot3(r, r);
+            const orc_real* xj = xstar + 3 * j;
+            const orc_real r[3] = {xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]};
+            const orc_real r2 = dot3(r, r);
             rho_i += poly6(p, r2); /* :140 */
-            double g[3];
+            orc_real g[3];
             grad_spiky(p, r, r2, g);
             sg += dot3(g, g) * ir2; /* :142-144 */
             gi[0] += g[0];
@@ -282,7 +282,7 @@ void orc_lambda(const orc_params* p, uint32_t n, const double* xstar, const uint
             gi[2] += g[2];
         });
         for (int a = 0; a < 3; ++a) gi[a] *= p->inv_rho0; /* :155 */
-        double C = rho_i / p->rho0 - 1.0;
+        orc_real C = rho_i / p->rho0 - 1.0;
         if (C < -p->cohesion) C = -p->cohesion; /* :156 */
         sg += dot3(gi, gi);                      /* :157 */
         lambda[i] = -C / (sg + p->eps);          /* :158 */
@@ -292,12 +292,12 @@ void orc_lambda(const orc_params* p, uint32_t n, const double* xstar, const uint
 
 /* Obstacle / container projection (CS_ApplyDeltaP.glsl:108-121,
  * CS_Integrate.glsl:216-240).  Returns 1 and the push normal on contact. */
-static int sdf_project(const orc_sdf* s, double x[3], double nrm[3])
+static int sdf_project(const orc_sdf* s, orc_real x[3], orc_real nrm[3])
 {
-    const double d = orc_sdf_query(s, x);
-    double g[3];
+    const orc_real d = orc_sdf_query(s, x);
+    orc_real g[3];
     orc_sdf_gradient(s, x, g);
-    const double len = sqrt(dot3(g, g));
+    const orc_real len = sqrt(dot3(g, g));
     if (!(len > 1e-6)) return 0;
     if (s->containment) {
         if (d > -s->padding) {
@@ -319,25 +319,25 @@ static int sdf_project(const orc_sdf* s, double x[3], double nrm[3])
     return 0;
 }
 
-void orc_deltap_apply(const orc_params* p, const orc_sdf* s, uint32_t n, double* xstar,
-                      const double* lambda, const uint32_t* ids, const int32_t* table,
-                      const uint32_t* lod, uint32_t iter, double* dp_out)
+void orc_deltap_apply(const orc_params* p, const orc_sdf* s, uint32_t n, orc_real* xstar,
+                      const orc_real* lambda, const uint32_t* ids, const int32_t* table,
+                      const uint32_t* lod, uint32_t iter, orc_real* dp_out)
 {
-    double* dp = dp_out ? dp_out : (double*)malloc(sizeof(double) * 3 * (size_t)n);
+    orc_real* dp = dp_out ? dp_out : (orc_real*)malloc(sizeof(orc_real) * 3 * (size_t)n);
     /* CS_ComputeDeltaP.glsl:120-166 */
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < (int64_t)n; ++i) {
         if (p->apbf && lod && lod[i] < iter) continue; /* :125 */
-        const double* xi = xstar + 3 * i;
-        const double li = lambda[i];
-        double acc[3] = {0, 0, 0};
+        const orc_real* xi = xstar + 3 * i;
+        const orc_real li = lambda[i];
+        orc_real acc[3] = {0, 0, 0};
         FOR_EACH_NEIGHBOUR(p, xi, i, ids, table, {
-            const double* xj = xstar + 3 * j;
-            const double r[3] = {xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]};
-            const double r2 = dot3(r, r);
-            double g[3];
+            const orc_real* xj = xstar + 3 * j;
+            const orc_real r[3] = {xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]};
+            const orc_real r2 = dot3(r, r);
+            orc_real g[3];
             grad_spiky(p, r, r2, g);
-            const double f = li + lambda[j] + scorr(p, r2); /* :155-156 */
+            const orc_real f = li + lambda[j] + scorr(p, r2); /* :155-156 */
             acc[0] += g[0] * f;
             acc[1] += g[1] * f;
             acc[2] += g[2] * f;
@@ -345,21 +345,21 @@ void orc_deltap_apply(const orc_params* p, const orc_sdf* s, uint32_t n, double*
         for (int a = 0; a < 3; ++a) dp[3 * i + a] = acc[a] * p->inv_rho0; /* :165 */
     }
     /* CS_ApplyDeltaP.glsl:80-124 */
-    const double maxdp = 0.5 * p->h;
+    const orc_real maxdp = 0.5 * p->h;
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < (int64_t)n; ++i) {
         if (p->apbf && lod && lod[i] < iter) continue; /* :85 */
-        double d[3] = {dp[3 * i], dp[3 * i + 1], dp[3 * i + 2]};
-        const double l2 = dot3(d, d);
+        orc_real d[3] = {dp[3 * i], dp[3 * i + 1], dp[3 * i + 2]};
+        const orc_real l2 = dot3(d, d);
         if (l2 > maxdp * maxdp) { /* :92-100 */
-            const double sc = maxdp / sqrt(l2);
+            const orc_real sc = maxdp / sqrt(l2);
             d[0] *= sc;
             d[1] *= sc;
             d[2] *= sc;
         }
-        double x[3] = {xstar[3 * i] + d[0], xstar[3 * i + 1] + d[1], xstar[3 * i + 2] + d[2]};
+        orc_real x[3] = {xstar[3 * i] + d[0], xstar[3 * i + 1] + d[1], xstar[3 * i + 2] + d[2]};
         if (s && s->enabled) {
-            double nrm[3];
+            orc_real nrm[3];
             sdf_project(s, x, nrm);
         }
         xstar[3 * i] = x[0];
@@ -369,33 +369,33 @@ void orc_deltap_apply(const orc_params* p, const orc_sdf* s, uint32_t n, double*
     if (!dp_out) free(dp);
 }
 
-void orc_integrate(const orc_params* p, const orc_sdf* s, uint32_t n, double* pos, double* vel,
-                   const double* xstar, const uint32_t* ids, const int32_t* table, double* omega)
+void orc_integrate(const orc_params* p, const orc_sdf* s, uint32_t n, orc_real* pos, orc_real* vel,
+                   const orc_real* xstar, const uint32_t* ids, const int32_t* table, orc_real* omega)
 {
     /* neighbour velocities are read from before the dispatch */
-    double* v0 = (double*)malloc(sizeof(double) * 3 * (size_t)n);
-    memcpy(v0, vel, sizeof(double) * 3 * (size_t)n);
-    const double inv_dt = (p->dt > 0.0) ? 1.0 / p->dt : 0.0; /* :244 */
+    orc_real* v0 = (orc_real*)malloc(sizeof(orc_real) * 3 * (size_t)n);
+    memcpy(v0, vel, sizeof(orc_real) * 3 * (size_t)n);
+    const orc_real inv_dt = (p->dt > 0.0) ? 1.0 / p->dt : 0.0; /* :244 */
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < (int64_t)n; ++i) {
-        const double* old_pos = pos + 3 * i;
-        const double* old_vel = v0 + 3 * i;
-        double x[3] = {xstar[3 * i], xstar[3 * i + 1], xstar[3 * i + 2]};
-        double visc_delta[3] = {0, 0, 0};
+        const orc_real* old_pos = pos + 3 * i;
+        const orc_real* old_vel = v0 + 3 * i;
+        orc_real x[3] = {xstar[3 * i], xstar[3 * i + 1], xstar[3 * i + 2]};
+        orc_real visc_delta[3] = {0, 0, 0};
         if (p->visc_on || p->vort_on) { /* :153-194 */
-            double vf[3] = {0, 0, 0}, curl[3] = {0, 0, 0};
+            orc_real vf[3] = {0, 0, 0}, curl[3] = {0, 0, 0};
             FOR_EACH_NEIGHBOUR(p, x, i, ids, table, {
-                const double* xj = xstar + 3 * j;
-                const double* vj = v0 + 3 * j;
-                const double r[3] = {x[0] - xj[0], x[1] - xj[1], x[2] - xj[2]};
-                const double r2 = dot3(r, r);
-                const double vij[3] = {vj[0] - old_vel[0], vj[1] - old_vel[1], vj[2] - old_vel[2]};
+                const orc_real* xj = xstar + 3 * j;
+                const orc_real* vj = v0 + 3 * j;
+                const orc_real r[3] = {x[0] - xj[0], x[1] - xj[1], x[2] - xj[2]};
+                const orc_real r2 = dot3(r, r);
+                const orc_real vij[3] = {vj[0] - old_vel[0], vj[1] - old_vel[1], vj[2] - old_vel[2]};
                 if (p->visc_on) {
-                    const double w = poly6(p, r2);
+                    const orc_real w = poly6(p, r2);
                     for (int a = 0; a < 3; ++a) vf[a] += vij[a] * w * p->inv_rho0; /* :177 */
                 }
                 if (p->vort_on) {
-                    double g[3];
+                    orc_real g[3];
                     grad_spiky(p, r, r2, g);
                     curl[0] += vij[1] * g[2] - vij[2] * g[1]; /* :182 */
                     curl[1] += vij[2] * g[0] - vij[0] * g[2];
@@ -413,19 +413,19 @@ void orc_integrate(const orc_params* p, const orc_sdf* s, uint32_t n, double* po
             if (x[a] >= p->bmax[a]) { x[a] = p->bmax[a]; col[a] = 1; }
         }
         int col_sdf = 0;
-        double nrm[3] = {0, 0, 0};
+        orc_real nrm[3] = {0, 0, 0};
         if (s && s->enabled) col_sdf = sdf_project(s, x, nrm); /* :216-240 */
-        double v[3];
+        orc_real v[3];
         for (int a = 0; a < 3; ++a) v[a] = (x[a] - old_pos[a]) * inv_dt + visc_delta[a]; /* :246,252 */
-        const double sp2 = dot3(v, v);
+        const orc_real sp2 = dot3(v, v);
         if (sp2 > 2500.0) { /* :255-256 */
-            const double sc = 50.0 / sqrt(sp2);
+            const orc_real sc = 50.0 / sqrt(sp2);
             for (int a = 0; a < 3; ++a) v[a] *= sc;
         }
         for (int a = 0; a < 3; ++a)
             if (col[a]) v[a] *= -p->damping; /* :259-261 */
         if (col_sdf) {                       /* :268-271 */
-            const double vn = dot3(v, nrm);
+            const orc_real vn = dot3(v, nrm);
             for (int a = 0; a < 3; ++a) v[a] -= vn * nrm[a];
         }
         for (int a = 0; a < 3; ++a) { /* :276-277 */
@@ -436,44 +436,44 @@ void orc_integrate(const orc_params* p, const orc_sdf* s, uint32_t n, double* po
     free(v0);
 }
 
-void orc_vorticity(const orc_params* p, uint32_t n, const double* pos, double* vel,
-                   const double* omega, const uint32_t* ids, const int32_t* table)
+void orc_vorticity(const orc_params* p, uint32_t n, const orc_real* pos, orc_real* vel,
+                   const orc_real* omega, const uint32_t* ids, const int32_t* table)
 {
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < (int64_t)n; ++i) {
-        const double* xi = pos + 3 * i;
-        double eta[3] = {0, 0, 0};
+        const orc_real* xi = pos + 3 * i;
+        orc_real eta[3] = {0, 0, 0};
         FOR_EACH_NEIGHBOUR(p, xi, i, ids, table, { /* :139-155 */
-            const double* xj = pos + 3 * j;
-            const double r[3] = {xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]};
-            const double r2 = dot3(r, r);
-            double g[3];
+            const orc_real* xj = pos + 3 * j;
+            const orc_real r[3] = {xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]};
+            const orc_real r2 = dot3(r, r);
+            orc_real g[3];
             grad_spiky(p, r, r2, g);
-            const double om = sqrt(dot3(omega + 3 * j, omega + 3 * j));
+            const orc_real om = sqrt(dot3(omega + 3 * j, omega + 3 * j));
             eta[0] += om * g[0];
             eta[1] += om * g[1];
             eta[2] += om * g[2];
         });
         for (int a = 0; a < 3; ++a) eta[a] *= p->inv_rho0; /* :157 */
-        const double el = sqrt(dot3(eta, eta));
+        const orc_real el = sqrt(dot3(eta, eta));
         if (el < 1e-6) continue; /* :160 */
-        const double N[3] = {eta[0] / el, eta[1] / el, eta[2] / el};
-        const double* w = omega + 3 * i;
-        const double cr[3] = {N[1] * w[2] - N[2] * w[1], N[2] * w[0] - N[0] * w[2], N[0] * w[1] - N[1] * w[0]};
+        const orc_real N[3] = {eta[0] / el, eta[1] / el, eta[2] / el};
+        const orc_real* w = omega + 3 * i;
+        const orc_real cr[3] = {N[1] * w[2] - N[2] * w[1], N[2] * w[0] - N[0] * w[2], N[0] * w[1] - N[1] * w[0]};
         for (int a = 0; a < 3; ++a) vel[3 * i + a] += p->vort_eps * cr[a] * p->dt; /* :166 */
     }
 }
 
-void orc_step(const orc_params* p, const orc_sdf* s, uint32_t n, double* pos, double* vel,
-              double* omega, double* rho, uint32_t* sorted_keys_out, uint32_t* sorted_ids_out,
+void orc_step(const orc_params* p, const orc_sdf* s, uint32_t n, orc_real* pos, orc_real* vel,
+              orc_real* omega, orc_real* rho, uint32_t* sorted_keys_out, uint32_t* sorted_ids_out,
               int32_t* table_out)
 {
     if (n == 0) return; /* PBFluids.cpp:325 */
     const uint32_t H = p->hash_size;
-    double* xs = (double*)malloc(sizeof(double) * 3 * (size_t)n);
-    double* lam = (double*)calloc((size_t)n, sizeof(double));
-    double* rh = (double*)malloc(sizeof(double) * (size_t)n);
-    double* om = (double*)calloc(3 * (size_t)n, sizeof(double));
+    orc_real* xs = (orc_real*)malloc(sizeof(orc_real) * 3 * (size_t)n);
+    orc_real* lam = (orc_real*)calloc((size_t)n, sizeof(orc_real));
+    orc_real* rh = (orc_real*)malloc(sizeof(orc_real) * (size_t)n);
+    orc_real* om = (orc_real*)calloc(3 * (size_t)n, sizeof(orc_real));
     uint32_t* keys = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)n);
     uint32_t* sk = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)n);
     uint32_t* ids = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)n);
@@ -484,7 +484,7 @@ void orc_step(const orc_params* p, const orc_sdf* s, uint32_t n, double* pos, do
 
     for (uint32_t sub = 0; sub < p->substeps; ++sub) { /* :344 */
         orc_predict(p, n, pos, vel, xs, keys);          /* :347-349 */
-        memset(lam, 0, sizeof(double) * (size_t)n);     /* CS_PredictAndHash.glsl:121 */
+        memset(lam, 0, sizeof(orc_real) * (size_t)n);     /* CS_PredictAndHash.glsl:121 */
         orc_stable_sort(keys, n, H, sk, ids);           /* :354-405 */
         orc_build_table(sk, n, H, table);               /* :408-418 */
         if (p->apbf) orc_lod(p, n, xs, lod);            /* :421-426 */
@@ -496,8 +496,8 @@ void orc_step(const orc_params* p, const orc_sdf* s, uint32_t n, double* pos, do
     }
     if (p->vort_on) orc_vorticity(p, n, pos, vel, om, ids, table); /* :499-505 */
 
-    if (omega) memcpy(omega, om, sizeof(double) * 3 * (size_t)n);
-    if (rho) memcpy(rho, rh, sizeof(double) * (size_t)n);
+    if (omega) memcpy(omega, om, sizeof(orc_real) * 3 * (size_t)n);
+    if (rho) memcpy(rho, rh, sizeof(orc_real) * (size_t)n);
     if (sorted_keys_out) memcpy(sorted_keys_out, sk, sizeof(uint32_t) * (size_t)n);
     if (sorted_ids_out) memcpy(sorted_ids_out, ids, sizeof(uint32_t) * (size_t)n);
     if (table_out) memcpy(table_out, table, sizeof(int32_t) * 2 * (size_t)H);
@@ -505,22 +505,22 @@ void orc_step(const orc_params* p, const orc_sdf* s, uint32_t n, double* pos, do
 }
 
 /* CS_ContactFilter.glsl:68-83 */
-uint32_t orc_contact_filter(const orc_sdf* s, uint32_t n, const double* pos, double band,
+uint32_t orc_contact_filter(const orc_sdf* s, uint32_t n, const orc_real* pos, orc_real band,
                             uint32_t* out_idx)
 {
     if (!s || !s->enabled || band <= 0.0) return 0; /* PBFluids.cpp:195 */
     uint32_t c = 0;
     for (uint32_t i = 0; i < n; ++i) {
-        const double d = orc_sdf_query(s, pos + 3 * i);
+        const orc_real d = orc_sdf_query(s, pos + 3 * i);
         if (fabs(d) < band) out_idx[c++] = i;
     }
     return c;
 }
 
 /* Kernel values for pinning against src/fluid/Kernels.cpp:9-27,116-141. */
-void orc_kernels(const orc_params* p, const double r[3], double* w, double g[3])
+void orc_kernels(const orc_params* p, const orc_real r[3], orc_real* w, orc_real g[3])
 {
-    const double r2 = dot3(r, r);
+    const orc_real r2 = dot3(r, r);
     *w = poly6(p, r2);
     grad_spiky(p, r, r2, g);
 }
@@ -528,16 +528,16 @@ void orc_kernels(const orc_params* p, const double r[3], double* w, double g[3])
 /* Visited candidates within h (r^2 <= h^2, with bucket multiplicity) — the
  * neighbour lists NeighborSearch::build (src/fluid/NeighborSearch.cpp:97-126)
  * produces when its cell size equals h. */
-void orc_neighbor_lists(const orc_params* p, uint32_t n, const double* x, const uint32_t* ids,
+void orc_neighbor_lists(const orc_params* p, uint32_t n, const orc_real* x, const uint32_t* ids,
                         const int32_t* table, int32_t* counts, int32_t* lists, int32_t cap)
 {
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < (int64_t)n; ++i) {
-        const double* xi = x + 3 * i;
+        const orc_real* xi = x + 3 * i;
         int32_t c = 0;
         FOR_EACH_NEIGHBOUR(p, xi, i, ids, table, {
-            const double* xj = x + 3 * j;
-            const double r[3] = {xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]};
+            const orc_real* xj = x + 3 * j;
+            const orc_real r[3] = {xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]};
             if (dot3(r, r) <= p->h2) {
                 if (lists && c < cap) lists[i * cap + c] = (int32_t)j;
                 ++c;

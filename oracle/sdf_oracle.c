@@ -14,17 +14,17 @@
 #include <stdlib.h>
 #include <string.h>
 
-typedef struct { double x, y, z; } d3;
-static inline d3 mk(double x, double y, double z) { d3 r = {x, y, z}; return r; }
+typedef struct { orc_real x, y, z; } d3;
+static inline d3 mk(orc_real x, orc_real y, orc_real z) { d3 r = {x, y, z}; return r; }
 static inline d3 sub(d3 a, d3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
 static inline d3 add(d3 a, d3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
-static inline d3 scl(d3 a, double s) { return mk(a.x * s, a.y * s, a.z * s); }
-static inline double dt3(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline d3 scl(d3 a, orc_real s) { return mk(a.x * s, a.y * s, a.z * s); }
+static inline orc_real dt3(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 static inline d3 crs(d3 a, d3 b) { return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
-static inline double nrm(d3 a) { return sqrt(dt3(a, a)); }
+static inline orc_real nrm(d3 a) { return sqrt(dt3(a, a)); }
 static inline d3 dmin(d3 a, d3 b) { return mk(fmin(a.x, b.x), fmin(a.y, b.y), fmin(a.z, b.z)); }
 static inline d3 dmax(d3 a, d3 b) { return mk(fmax(a.x, b.x), fmax(a.y, b.y), fmax(a.z, b.z)); }
-static inline double comp(d3 a, int k) { return k == 0 ? a.x : (k == 1 ? a.y : a.z); }
+static inline orc_real comp(d3 a, int k) { return k == 0 ? a.x : (k == 1 ? a.y : a.z); }
 
 /* Feature enum (SDFBoundary.cpp:17) */
 enum { F_FACE, F_EDGE_AB, F_EDGE_AC, F_EDGE_BC, F_VA, F_VB, F_VC };
@@ -33,24 +33,24 @@ enum { F_FACE, F_EDGE_AB, F_EDGE_AC, F_EDGE_BC, F_VA, F_VB, F_VC };
 static d3 closest_on_tri(d3 P, d3 A, d3 B, d3 C, int* feature)
 {
     const d3 AB = sub(B, A), AC = sub(C, A), AP = sub(P, A);
-    const double d1 = dt3(AB, AP), d2 = dt3(AC, AP);
+    const orc_real d1 = dt3(AB, AP), d2 = dt3(AC, AP);
     if (d1 <= 0 && d2 <= 0) { *feature = F_VA; return A; }
     const d3 BP = sub(P, B);
-    const double d3_ = dt3(AB, BP), d4 = dt3(AC, BP);
+    const orc_real d3_ = dt3(AB, BP), d4 = dt3(AC, BP);
     if (d3_ >= 0 && d4 <= d3_) { *feature = F_VB; return B; }
     const d3 CP = sub(P, C);
-    const double d5 = dt3(AB, CP), d6 = dt3(AC, CP);
+    const orc_real d5 = dt3(AB, CP), d6 = dt3(AC, CP);
     if (d6 >= 0 && d5 <= d6) { *feature = F_VC; return C; }
-    const double vc = d1 * d4 - d3_ * d2;
+    const orc_real vc = d1 * d4 - d3_ * d2;
     if (vc <= 0 && d1 >= 0 && d3_ <= 0) { *feature = F_EDGE_AB; return add(A, scl(AB, d1 / (d1 - d3_))); }
-    const double vb = d5 * d2 - d1 * d6;
+    const orc_real vb = d5 * d2 - d1 * d6;
     if (vb <= 0 && d2 >= 0 && d6 <= 0) { *feature = F_EDGE_AC; return add(A, scl(AC, d2 / (d2 - d6))); }
-    const double va = d3_ * d6 - d5 * d4;
+    const orc_real va = d3_ * d6 - d5 * d4;
     if (va <= 0 && (d4 - d3_) >= 0 && (d5 - d6) >= 0) {
         *feature = F_EDGE_BC;
         return add(B, scl(sub(C, B), (d4 - d3_) / ((d4 - d3_) + (d5 - d6))));
     }
-    const double denom = 1.0 / (va + vb + vc);
+    const orc_real denom = 1.0 / (va + vb + vc);
     *feature = F_FACE;
     return add(A, add(scl(AB, vb * denom), scl(AC, vc * denom)));
 }
@@ -77,17 +77,17 @@ struct orc_mesh {
     int* order;
     d3 *tmin, *tmax, *cen;
     /* grid */
-    double origin[3], cell;
+    orc_real origin[3], cell;
     int dims[3];
 };
 
-static void tri_set(tri_t* t, const double* v)
+static void tri_set(tri_t* t, const orc_real* v)
 {
     t->A = mk(v[3 * t->iA], v[3 * t->iA + 1], v[3 * t->iA + 2]);
     t->B = mk(v[3 * t->iB], v[3 * t->iB + 1], v[3 * t->iB + 2]);
     t->C = mk(v[3 * t->iC], v[3 * t->iC + 1], v[3 * t->iC + 2]);
     d3 n = crs(sub(t->B, t->A), sub(t->C, t->A));
-    const double len = nrm(n);
+    const orc_real len = nrm(n);
     if (len > 1e-12) n = scl(n, 1.0 / len);
     t->fn = n;
 }
@@ -98,7 +98,7 @@ static void nth_select(struct orc_mesh* m, int lo, int hi, int nth, int axis)
 {
     int* o = m->order;
     while (hi - lo > 1) {
-        const double pv = comp(m->cen[o[lo + (hi - lo) / 2]], axis);
+        const orc_real pv = comp(m->cen[o[lo + (hi - lo) / 2]], axis);
         int i = lo, j = hi - 1;
         while (i <= j) {
             while (comp(m->cen[o[i]], axis) < pv) ++i;
@@ -162,7 +162,7 @@ static int edge_cmp(const void* x, const void* y)
     return e->t < f->t ? -1 : (e->t > f->t);
 }
 
-orc_mesh* orc_mesh_build(const double* verts, int32_t nv, const int32_t* faces, int32_t nf, double cell)
+orc_mesh* orc_mesh_build(const orc_real* verts, int32_t nv, const int32_t* faces, int32_t nf, orc_real cell)
 {
     struct orc_mesh* m = (struct orc_mesh*)calloc(1, sizeof(struct orc_mesh));
     m->nv = nv;
@@ -174,12 +174,12 @@ orc_mesh* orc_mesh_build(const double* verts, int32_t nv, const int32_t* faces, 
         bmin = dmin(bmin, v);
         bmax = dmax(bmax, v);
     }
-    const double buffer = cell * 5.0;
+    const orc_real buffer = cell * 5.0;
     m->origin[0] = bmin.x - buffer;
     m->origin[1] = bmin.y - buffer;
     m->origin[2] = bmin.z - buffer;
     m->cell = cell;
-    const double span[3] = {(bmax.x + buffer) - m->origin[0], (bmax.y + buffer) - m->origin[1],
+    const orc_real span[3] = {(bmax.x + buffer) - m->origin[0], (bmax.y + buffer) - m->origin[1],
                             (bmax.z + buffer) - m->origin[2]};
     for (int k = 0; k < 3; ++k) m->dims[k] = (int)ceil(span[k] / cell);
 
@@ -202,18 +202,18 @@ orc_mesh* orc_mesh_build(const double* verts, int32_t nv, const int32_t* faces, 
         for (int c = 0; c < 3; ++c) {
             const d3 vtx = P[c], p1 = P[(c + 1) % 3], p2 = P[(c + 2) % 3];
             d3 a = sub(p1, vtx), b = sub(p2, vtx);
-            const double la = nrm(a), lb = nrm(b);
+            const orc_real la = nrm(a), lb = nrm(b);
             /* Eigen normalized() leaves a zero vector unchanged */
             if (la > 0) a = scl(a, 1.0 / la);
             if (lb > 0) b = scl(b, 1.0 / lb);
-            double cs = dt3(a, b);
+            orc_real cs = dt3(a, b);
             cs = cs < -1.0 ? -1.0 : (cs > 1.0 ? 1.0 : cs);
-            const double ang = acos(cs);
+            const orc_real ang = acos(cs);
             m->vn[iv[c]] = add(m->vn[iv[c]], scl(t->fn, ang));
         }
     }
     for (int i = 0; i < nv; ++i) {
-        const double len = nrm(m->vn[i]);
+        const orc_real len = nrm(m->vn[i]);
         if (len > 1e-12) m->vn[i] = scl(m->vn[i], 1.0 / len);
     }
     /* edge pseudo-normals: average of exactly two incident faces (:361-383) */
@@ -233,7 +233,7 @@ orc_mesh* orc_mesh_build(const double* verts, int32_t nv, const int32_t* faces, 
         while (j < 3 * (size_t)nf && e[j].a == e[i].a && e[j].b == e[i].b) ++j;
         if (j - i == 2) {
             const d3 s = add(m->tris[e[i].t].fn, m->tris[e[i + 1].t].fn);
-            const double len = nrm(s);
+            const orc_real len = nrm(s);
             if (len >= 1e-12) {
                 const d3 en = scl(s, 1.0 / len);
                 for (size_t k = i; k < j; ++k) {
@@ -275,7 +275,7 @@ void orc_mesh_free(orc_mesh* m)
 }
 
 /* updateGeometryAndRefit + TriangleBVH::refit (SDFBoundary.cpp:120-148,438-453) */
-void orc_mesh_refit(orc_mesh* m, const double* verts)
+void orc_mesh_refit(orc_mesh* m, const orc_real* verts)
 {
     for (int f = 0; f < m->nf; ++f) tri_set(&m->tris[f], verts);
     tri_aabbs(m);
@@ -296,21 +296,21 @@ void orc_mesh_refit(orc_mesh* m, const double* verts)
     }
 }
 
-void orc_mesh_grid_info(const orc_mesh* m, int32_t dims[3], double origin[3], double* cell)
+void orc_mesh_grid_info(const orc_mesh* m, int32_t dims[3], orc_real origin[3], orc_real* cell)
 {
     for (int k = 0; k < 3; ++k) { dims[k] = m->dims[k]; origin[k] = m->origin[k]; }
     *cell = m->cell;
 }
 
-typedef struct { double dist2; d3 point; int feature, tri; } hit_t;
+typedef struct { orc_real dist2; d3 point; int feature, tri; } hit_t;
 
-static double sq_dist_aabb(d3 p, d3 bmin, d3 bmax)
+static orc_real sq_dist_aabb(d3 p, d3 bmin, d3 bmax)
 {
-    double d2 = 0.0;
+    orc_real d2 = 0.0;
     for (int i = 0; i < 3; ++i) {
-        const double v = comp(p, i), lo = comp(bmin, i), hi = comp(bmax, i);
-        if (v < lo) { const double t = lo - v; d2 += t * t; }
-        else if (v > hi) { const double t = v - hi; d2 += t * t; }
+        const orc_real v = comp(p, i), lo = comp(bmin, i), hi = comp(bmax, i);
+        if (v < lo) { const orc_real t = lo - v; d2 += t * t; }
+        else if (v > hi) { const orc_real t = v - hi; d2 += t * t; }
     }
     return d2;
 }
@@ -327,7 +327,7 @@ static void query(const struct orc_mesh* m, int ni, d3 P, hit_t* best)
             int feat;
             const d3 cp = closest_on_tri(P, tr->A, tr->B, tr->C, &feat);
             const d3 dd = sub(P, cp);
-            const double d2 = dt3(dd, dd);
+            const orc_real d2 = dt3(dd, dd);
             if (d2 < best->dist2) {
                 best->dist2 = d2;
                 best->point = cp;
@@ -337,8 +337,8 @@ static void query(const struct orc_mesh* m, int ni, d3 P, hit_t* best)
         }
         return;
     }
-    const double dL = sq_dist_aabb(P, m->nodes[nd->left].bmin, m->nodes[nd->left].bmax);
-    const double dR = sq_dist_aabb(P, m->nodes[nd->right].bmin, m->nodes[nd->right].bmax);
+    const orc_real dL = sq_dist_aabb(P, m->nodes[nd->left].bmin, m->nodes[nd->left].bmax);
+    const orc_real dR = sq_dist_aabb(P, m->nodes[nd->right].bmin, m->nodes[nd->right].bmax);
     if (dL <= dR) {
         if (dL < best->dist2) query(m, nd->left, P, best);
         if (dR < best->dist2) query(m, nd->right, P, best);
@@ -360,7 +360,7 @@ static hit_t closest(const struct orc_mesh* m, d3 P)
 }
 
 /* signedDistanceAt (SDFBoundary.cpp:400-419) */
-double orc_mesh_signed_distance(const orc_mesh* m, const double p[3])
+orc_real orc_mesh_signed_distance(const orc_mesh* m, const orc_real p[3])
 {
     const d3 P = mk(p[0], p[1], p[2]);
     const hit_t h = closest(m, P);
@@ -376,7 +376,7 @@ double orc_mesh_signed_distance(const orc_mesh* m, const double p[3])
     case F_VB: pn = m->vn[t->iB]; break;
     default: pn = m->vn[t->iC]; break;
     }
-    const double sign = (dt3(sub(P, h.point), pn) >= 0.0) ? 1.0 : -1.0;
+    const orc_real sign = (dt3(sub(P, h.point), pn) >= 0.0) ? 1.0 : -1.0;
     return sign * sqrt(h.dist2);
 }
 
@@ -388,13 +388,13 @@ void orc_mesh_grid(const orc_mesh* m, float* out)
     for (int x = 0; x < dx; ++x)
         for (int y = 0; y < dy; ++y)
             for (int z = 0; z < dz; ++z) {
-                const double P[3] = {m->origin[0] + x * m->cell, m->origin[1] + y * m->cell,
+                const orc_real P[3] = {m->origin[0] + x * m->cell, m->origin[1] + y * m->cell,
                                      m->origin[2] + z * m->cell};
                 out[((int64_t)x * dy + y) * dz + z] = (float)orc_mesh_signed_distance(m, P);
             }
 }
 
-int32_t orc_mesh_closest(const orc_mesh* m, const double p[3], double point[3], double* dist2)
+int32_t orc_mesh_closest(const orc_mesh* m, const orc_real p[3], orc_real point[3], orc_real* dist2)
 {
     const hit_t h = closest(m, mk(p[0], p[1], p[2]));
     point[0] = h.point.x;
@@ -405,19 +405,19 @@ int32_t orc_mesh_closest(const orc_mesh* m, const double p[3], double point[3], 
 }
 
 /* barycentric, clamped and renormalised (src/main.cpp:557-571) */
-static void barycentric(d3 Pt, d3 A, d3 B, d3 C, double* u, double* v, double* w)
+static void barycentric(d3 Pt, d3 A, d3 B, d3 C, orc_real* u, orc_real* v, orc_real* w)
 {
     const d3 v0 = sub(B, A), v1 = sub(C, A), v2 = sub(Pt, A);
-    const double d00 = dt3(v0, v0), d01 = dt3(v0, v1), d11 = dt3(v1, v1);
-    const double d20 = dt3(v2, v0), d21 = dt3(v2, v1);
-    const double denom = d00 * d11 - d01 * d01;
+    const orc_real d00 = dt3(v0, v0), d01 = dt3(v0, v1), d11 = dt3(v1, v1);
+    const orc_real d20 = dt3(v2, v0), d21 = dt3(v2, v1);
+    const orc_real denom = d00 * d11 - d01 * d01;
     if (fabs(denom) < 1e-20) { *u = 1; *v = 0; *w = 0; return; }
-    const double vv = (d11 * d20 - d01 * d21) / denom;
-    const double ww = (d00 * d21 - d01 * d20) / denom;
-    double uu = 1.0 - vv - ww;
+    const orc_real vv = (d11 * d20 - d01 * d21) / denom;
+    const orc_real ww = (d00 * d21 - d01 * d20) / denom;
+    orc_real uu = 1.0 - vv - ww;
     uu = fmax(0.0, uu);
-    double vc = fmax(0.0, vv), wc = fmax(0.0, ww);
-    const double s = uu + vc + wc;
+    orc_real vc = fmax(0.0, vv), wc = fmax(0.0, ww);
+    const orc_real s = uu + vc + wc;
     if (s > 1e-20) { uu /= s; vc /= s; wc /= s; }
     *u = uu; *v = vc; *w = wc;
 }
@@ -426,9 +426,9 @@ static void barycentric(d3 Pt, d3 A, d3 B, d3 C, double* u, double* v, double* w
  * triangle, skip beyond band, push direction, velocity-into-surface magnitude,
  * barycentric split.  Summed in candidate order. */
 int32_t orc_contact_forces(const orc_mesh* m, const pbf_contact_candidate* cand, uint32_t count,
-                           double band, int use_vel, double* forces)
+                           orc_real band, int use_vel, orc_real* forces)
 {
-    memset(forces, 0, sizeof(double) * 3 * (size_t)m->nv);
+    memset(forces, 0, sizeof(orc_real) * 3 * (size_t)m->nv);
     int32_t contacts = 0;
     for (uint32_t c = 0; c < count; ++c) {
         const d3 P = mk(cand[c].pos[0], cand[c].pos[1], cand[c].pos[2]);
@@ -436,27 +436,27 @@ int32_t orc_contact_forces(const orc_mesh* m, const pbf_contact_candidate* cand,
         const hit_t h = closest(m, P); /* :637 */
         if (h.tri < 0) continue;
         const d3 to = sub(h.point, P);
-        const double dist = nrm(to);
+        const orc_real dist = nrm(to);
         if (dist > band) continue; /* :642 */
         const tri_t* t = &m->tris[h.tri];
         d3 dir;
         if (dist > 1e-6) dir = scl(to, 1.0 / dist); /* :651-657 */
         else {
             d3 n = crs(sub(t->B, t->A), sub(t->C, t->A));
-            const double l = nrm(n);
+            const orc_real l = nrm(n);
             if (l > 0) n = scl(n, 1.0 / l);
             dir = scl(n, -1.0);
         }
-        double mag = 1.0;
+        orc_real mag = 1.0;
         if (use_vel) { /* :661-665 */
             mag = fmax(0.0, dt3(vel, dir));
             if (mag <= 0.0) continue;
         }
-        double u, v, w;
+        orc_real u, v, w;
         barycentric(h.point, t->A, t->B, t->C, &u, &v, &w); /* :667-669 */
         const d3 F = scl(dir, mag);
         const int iv[3] = {t->iA, t->iB, t->iC};
-        const double wt[3] = {u, v, w};
+        const orc_real wt[3] = {u, v, w};
         for (int k = 0; k < 3; ++k) { /* :671-673 */
             forces[3 * iv[k]] += F.x * wt[k];
             forces[3 * iv[k] + 1] += F.y * wt[k];
