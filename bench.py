@@ -34,9 +34,17 @@ sys.path.insert(0, os.path.join(ROOT, "realtime-fsi-engine_b200"))
 
 METRIC = "particle-substeps/s"
 # algorithmic bytes per particle and launch (payload only: vec3 = 12 B,
-# scalar = 4 B; each pass reads its inputs and writes its outputs once)
+# scalar = 4 B; each pass reads its inputs and writes its outputs once); the
+# cell table also clears its H buckets of 8 B each, 8 H / N per particle
 ALGO_BYTES = {"predict_hash": 28, "radix_sort": 16, "cell_table": 12, "reorder": 64, "lambda": 16,
               "deltap_apply": 28, "integrate": 72, "vorticity": 48}
+
+
+def algo_bytes(name, n, hash_size):
+    b = ALGO_BYTES.get(name, 0) * n
+    if name == "cell_table":
+        b += 8 * hash_size
+    return b
 
 
 def parse():
@@ -369,7 +377,7 @@ def run_b200(args, dist):
         if name == "step" or cnt == 0:
             continue
         per_launch = pms / cnt
-        b = ALGO_BYTES.get(name, 0) * n
+        b = algo_bytes(name, n, cfg.hash_size)
         per_pass[name] = {"ms_total": round(pms, 4), "launches": int(cnt), "ms_per_launch": round(per_launch, 5),
                           "share": round(pms / max(sum(v[0] for k, v in passes.items() if k != "step"), 1e-9), 4),
                           "algo_bytes_per_launch": b,
