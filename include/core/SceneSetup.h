@@ -34,7 +34,8 @@ struct MeshData {
 // each vertex line are its position (normals, colours after them are
 // ignored), polygons are fan-triangulated from their first vertex.  Returns
 // false (and leaves `out` untouched) when the file cannot be opened, is not
-// an OFF file, or ends before the counts it declares.
+// an OFF file, ends before the counts it declares, or names a vertex index
+// outside [0, vertex count) or a polygon of more than 4096 vertices.
 bool loadOFF(const std::string& path, MeshData& out);
 
 // Centres the mesh's bounding box on `center` and scales its largest extent

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <exception>
 #include <fstream>
 #include <random>
 #include <sstream>
@@ -157,24 +158,27 @@ bool loadOFF(const std::string& path, MeshData& out)
         }
         nv = nf = -1;
     }
-    if (nv < 0 || nf < 0) return false;
+    // counts past 2^30 are malformed; storage grows with the lines actually
+    // read, so a count larger than the file allocates nothing up front
+    if (nv < 0 || nf < 0 || nv > (1L << 30) || nf > (1L << 30)) return false;
     MeshData m;
-    m.verts.resize((size_t)nv);
     for (long i = 0; i < nv; ++i) {
         if (!next_content_line(f, line)) return false;
         std::istringstream ss(line);
         double x = 0.0, y = 0.0, z = 0.0;
         ss >> x >> y >> z;
-        m.verts[(size_t)i] = {x, y, z};
+        m.verts.push_back({x, y, z});
     }
-    m.faces.reserve((size_t)nf);
     for (long i = 0; i < nf; ++i) {
         if (!next_content_line(f, line)) return false;
         std::istringstream ss(line);
         int k = 0;
         ss >> k;
-        std::vector<int> poly((size_t)std::max(k, 0));
-        for (auto& q : poly) ss >> q;
+        if (k < 0 || k > 4096) return false;  // a polygon's vertex count
+        std::vector<int> poly((size_t)k);
+        for (auto& q : poly) {
+            if (!(ss >> q) || q < 0 || q >= nv) return false;  // a missing or out-of-range vertex index
+        }
         for (int j = 1; j + 1 < k; ++j) m.faces.push_back({poly[0], poly[(size_t)j], poly[(size_t)j + 1]});
     }
     out = std::move(m);
@@ -387,7 +391,11 @@ extern "C" int pbf_off_load(const char* path, double* verts3, int32_t vcap, int3
 {
     if (!path || !nv || !nf) return set_error(PBF_ERR_INVALID, "null argument");
     MeshData m;
-    if (!loadOFF(path, m)) return set_error(PBF_ERR_INVALID, "pbf_off_load: cannot read an OFF mesh from %s", path);
+    try {
+        if (!loadOFF(path, m)) return set_error(PBF_ERR_INVALID, "pbf_off_load: cannot read an OFF mesh from %s", path);
+    } catch (const std::exception& e) {
+        return set_error(PBF_ERR_ALLOC, "pbf_off_load: %s", e.what());
+    }
     if (m.verts.size() > (size_t)INT32_MAX || m.faces.size() > (size_t)INT32_MAX)
         return set_error(PBF_ERR_INVALID, "pbf_off_load: mesh too large");
     *nv = (int32_t)m.verts.size();
@@ -419,9 +427,13 @@ void unwrap(const MeshData& m, double* verts3)
 extern "C" int pbf_mesh_fit(double* verts3, int32_t nv, const float center[3], double target_size)
 {
     if (!verts3 || !center || nv < 0) return set_error(PBF_ERR_INVALID, "bad mesh arguments");
-    MeshData m = wrap(verts3, nv);
-    fitMeshToDomain(m, PVec3{center[0], center[1], center[2]}, target_size);
-    unwrap(m, verts3);
+    try {
+        MeshData m = wrap(verts3, nv);
+        fitMeshToDomain(m, PVec3{center[0], center[1], center[2]}, target_size);
+        unwrap(m, verts3);
+    } catch (const std::exception& e) {
+        return set_error(PBF_ERR_ALLOC, "pbf_mesh_fit: %s", e.what());
+    }
     return PBF_OK;
 }
 
@@ -436,16 +448,25 @@ extern "C" int pbf_mesh_fit_center(const pbf_fluid_config* cfg, float center_out
 extern "C" int pbf_mesh_place(double* verts3, int32_t nv, const float translate[3], const float rot_deg[3])
 {
     if (!verts3 || !translate || !rot_deg || nv < 0) return set_error(PBF_ERR_INVALID, "bad mesh arguments");
-    MeshData m = wrap(verts3, nv);
-    placeMesh(m, PVec3{translate[0], translate[1], translate[2]}, PVec3{rot_deg[0], rot_deg[1], rot_deg[2]});
-    unwrap(m, verts3);
+    try {
+        MeshData m = wrap(verts3, nv);
+        placeMesh(m, PVec3{translate[0], translate[1], translate[2]}, PVec3{rot_deg[0], rot_deg[1], rot_deg[2]});
+        unwrap(m, verts3);
+    } catch (const std::exception& e) {
+        return set_error(PBF_ERR_ALLOC, "pbf_mesh_place: %s", e.what());
+    }
     return PBF_OK;
 }
 
 extern "C" int pbf_spawn_particles(const pbf_fluid_config* cfg, pbf_particle* out, uint32_t capacity, uint32_t* count)
 {
     if (!cfg || !count) return set_error(PBF_ERR_INVALID, "null argument");
-    const std::vector<Particle> ps = spawnParticles(pbfhost::fluid_config_from_c(*cfg));
+    std::vector<Particle> ps;
+    try {
+        ps = spawnParticles(pbfhost::fluid_config_from_c(*cfg));
+    } catch (const std::exception& e) {
+        return set_error(PBF_ERR_ALLOC, "pbf_spawn_particles: %s", e.what());
+    }
     *count = (uint32_t)ps.size();
     if (out && capacity >= *count) std::memcpy(out, ps.data(), ps.size() * sizeof(Particle));
     return PBF_OK;

@@ -126,7 +126,11 @@ def test_off_reader_rejects_bad_files(tmp_path):
     bad.write_text("PLY\n3 1 0\n")
     short = tmp_path / "short.off"
     short.write_text("OFF\n4 2 0\n0 0 0\n1 0 0\n")
-    for path in (bad, short, tmp_path / "missing.off"):
+    oob = tmp_path / "oob.off"
+    oob.write_text("OFF\n3 1 0\n0 0 0\n1 0 0\n0 1 0\n3 0 1 3\n")
+    huge = tmp_path / "huge.off"
+    huge.write_text("OFF\n3 1 0\n0 0 0\n1 0 0\n0 1 0\n2000000000 0 1 2\n")
+    for path in (bad, short, oob, huge, tmp_path / "missing.off"):
         with pytest.raises(PBFError):
             presets.load_off(str(path))
 
