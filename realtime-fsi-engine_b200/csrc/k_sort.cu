@@ -17,8 +17,8 @@
 namespace pbf {
 
 constexpr int kSortThreads = 256;
-constexpr int kSortItems = 16;
-constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
+constexpr int kSortItems = 8;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys per tile
 static_assert(kSortTile == (int)kSortTileKeys, "scratch sizing elsewhere uses kSortTileKeys");
 constexpr int kRadix = 256;
 constexpr int kWarps = kSortThreads / 32;
@@ -34,10 +34,18 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_upsweep(const uint32_t* _
     for (int i = threadIdx.x; i < kWarps * kRadix; i += kSortThreads) (&cnt[0][0])[i] = 0;
     __syncthreads();
     const uint32_t base = blockIdx.x * kSortTile;
-#pragma unroll 4
+    // all of the thread's loads are issued before its first shared-memory
+    // atomic, so they are in flight together
+    uint32_t k[kSortItems];
+#pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
         const uint32_t idx = base + r * kSortThreads + threadIdx.x;
-        if (idx < n) atomicAdd(&cnt[warp][(__ldg(keys + idx) >> shift) & dmask], 1u);
+        k[r] = idx < n ? __ldg(keys + idx) : 0xffffffffu;
+    }
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const uint32_t idx = base + r * kSortThreads + threadIdx.x;
+        if (idx < n) atomicAdd(&cnt[warp][(k[r] >> shift) & dmask], 1u);
     }
     __syncthreads();
     for (int d = threadIdx.x; d < kRadix; d += kSortThreads) {
@@ -139,7 +147,7 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_downsweep(
     for (int i = threadIdx.x; i < kWarps * kRadix; i += kSortThreads) (&s_wcnt[0][0])[i] = 0;
     __syncthreads();
 
-    // load: warp w owns items [w*512, w*512+512) of the tile, round-major
+    // load: warp w owns items [w*32*kSortItems, (w+1)*32*kSortItems) of the tile, round-major
     uint32_t key[kSortItems], id[kSortItems], rank[kSortItems];
     const uint32_t wbase = base + warp * (32 * kSortItems);
 #pragma unroll

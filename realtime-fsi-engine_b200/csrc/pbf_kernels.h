@@ -104,7 +104,7 @@ void launch_d_unpermute1(uint32_t n, const uint32_t* inv, const float* src, floa
 // ---- k_sort.cu ----------------------------------------------------------------
 // Keys per sort tile: one 256-digit histogram per tile, so scratch sized for
 // n keys holds 256 * sort_num_tiles(n) histogram words.
-constexpr uint32_t kSortTileKeys = 4096;
+constexpr uint32_t kSortTileKeys = 2048;
 uint32_t sort_num_tiles(uint32_t n);
 void launch_radix_sort(uint32_t n, uint32_t key_bits, const uint32_t* keys_in, uint32_t* ka, uint32_t* ia,
                        uint32_t* kb, uint32_t* ib, uint32_t* hist, uint32_t* totals, uint32_t** out_keys,
