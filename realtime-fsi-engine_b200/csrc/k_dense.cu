@@ -58,6 +58,7 @@
 #include "masked_body.cuh"
 #include "pbf_batch.h"
 #include "pbf_kernels.h"
+#include <type_traits>
 
 namespace pbf {
 
@@ -321,7 +322,7 @@ template <int C, class Hit, class Body, class Rec = NoRecord>
 __device__ __forceinline__ void label_range(const float4* __restrict__ X, float4 xi, int self, int lo, int hi,
                                             Hit&& hit, Body&& body, Rec&& rec = Rec{})
 {
-    static_assert(C >= 1 && C <= 32, "hit mask is 32 bits");
+    static_assert(C >= 4 && C <= 32 && C % 4 == 0, "hit mask is 32 bits; chunks test in quarters");
     constexpr int G = 32 / C;  // chunks tested before one drain of up to 32 candidates
     const float2 xy = make_float2(xi.x, xi.y);
 #pragma unroll 1
@@ -332,13 +333,29 @@ __device__ __forceinline__ void label_range(const float4* __restrict__ X, float4
             const int kb = k0 + g * C;
             if (kb >= hi) break;
             uint32_t mg = 0;
+            // a run's last chunk is tested only as far as the warp's lanes
+            // still have candidates (in quarters of the chunk: the lanes of a
+            // warp mostly share their runs): candidates past a lane's run end
+            // are masked below, so the mask is the same as a whole chunk's
+            const int need = (int)__reduce_max_sync(__activemask(), (uint32_t)min(hi - kb, C));
+            auto test = [&](auto NC) {
+                constexpr int N = decltype(NC)::value;
 #pragma unroll
-            for (int c = 0; c < C; ++c) {
-                const float4 xj = __ldg(X + kb + c);
-                const float2 rxy = sub_f32x2(xy, make_float2(xj.x, xj.y));
-                const float rx = rxy.x, ry = rxy.y, rz = xi.z - xj.z;
-                if (hit(rx * rx + ry * ry + rz * rz)) mg |= 1u << c;
-            }
+                for (int c = 0; c < N; ++c) {
+                    const float4 xj = __ldg(X + kb + c);
+                    const float2 rxy = sub_f32x2(xy, make_float2(xj.x, xj.y));
+                    const float rx = rxy.x, ry = rxy.y, rz = xi.z - xj.z;
+                    if (hit(rx * rx + ry * ry + rz * rz)) mg |= 1u << c;
+                }
+            };
+            if (need > (3 * C) / 4)
+                test(std::integral_constant<int, C>{});
+            else if (need > C / 2)
+                test(std::integral_constant<int, (3 * C) / 4>{});
+            else if (need > C / 4)
+                test(std::integral_constant<int, C / 2>{});
+            else
+                test(std::integral_constant<int, C / 4>{});
             const uint32_t ds = (uint32_t)(self - kb);
             if (ds < (uint32_t)C) mg &= ~(1u << ds);
             const int left = hi - kb;
