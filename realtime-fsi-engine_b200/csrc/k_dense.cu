@@ -144,6 +144,34 @@ __global__ void __launch_bounds__(256) k_d_keys_pred(DevParams P0, DenseArgs D0,
     }
 }
 
+// The predict pass of one scene in mode 8: k_predict_hash's hash key of each
+// particle's predict-time cell (particle order) and, from the same x*, the
+// window slot of that cell, so that the relabelling gathers a 4-byte key by id
+// instead of re-deriving x* from the particle state.
+__global__ void __launch_bounds__(256) k_d_predict_hash(DevParams P, DenseArgs D, const float4* __restrict__ pos,
+                                                        const float4* __restrict__ vel, uint32_t* __restrict__ keys,
+                                                        uint32_t* __restrict__ dkey_id)
+{
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += stride) {
+        float3 vp, xs;
+        predict_particle(P, __ldg(pos + i), __ldg(vel + i), vp, xs);
+        const int cx = cell_coord(xs.x, P.h), cy = cell_coord(xs.y, P.h), cz = cell_coord(xs.z, P.h);
+        keys[i] = grid_hash(cx, cy, cz, P.mask);
+        dkey_id[i] = dense_key(D, cx, cy, cz);
+    }
+}
+
+// dkey[s] = the window slot of hash-sorted particle ids[s], from k_d_predict_hash.
+__global__ void __launch_bounds__(256) k_d_keys_gather(uint32_t n, const uint32_t* __restrict__ ids,
+                                                       const uint32_t* __restrict__ dkey_id,
+                                                       uint32_t* __restrict__ dkey)
+{
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += stride)
+        dkey[s] = __ldg(dkey_id + __ldg(ids + s));
+}
+
 // Label t = hash-sorted index order[t]: its x* (also the predict-time copy),
 // predicted velocity, substep-start position, id and key, gathered from the
 // particle state (the predict pass's arithmetic again), and inv[order[t]] = t.
@@ -998,6 +1026,18 @@ void launch_d_keys_pred(const DevParams& P, const DenseArgs& D, const uint32_t* 
                         const float4* vel, uint32_t* dkey, int sms, cudaStream_t st)
 {
     PBF_DENSE_LAUNCH(k_d_keys_pred, capped_grid(P.n, 256, sms, 8), 256, P, D, ids, pos, vel, dkey);
+}
+
+void launch_d_predict_hash(const DevParams& P, const DenseArgs& D, const float4* pos, const float4* vel,
+                           uint32_t* keys, uint32_t* dkey_id, int sms, cudaStream_t st)
+{
+    k_d_predict_hash<<<capped_grid(P.n, 256, sms, 8), 256, 0, st>>>(P, D, pos, vel, keys, dkey_id);
+}
+
+void launch_d_keys_gather(uint32_t n, const uint32_t* ids, const uint32_t* dkey_id, uint32_t* dkey, int sms,
+                          cudaStream_t st)
+{
+    k_d_keys_gather<<<capped_grid(n, 256, sms, 8), 256, 0, st>>>(n, ids, dkey_id, dkey);
 }
 
 void launch_d_permute(const DevParams& P, const uint32_t* order, const uint32_t* ids, const uint32_t* skeys,

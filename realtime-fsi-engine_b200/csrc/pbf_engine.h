@@ -77,6 +77,15 @@ struct pbf_handle {
     uint32_t dwin_mask = 0;
     bool dwin_ready = false;
     uint32_t dwin_unclean = 0;
+    // mode 8: the predict pass's window slot of each particle (particle order),
+    // valid for the next relabelling when neither the particles (particles_gen),
+    // the parameters nor the window changed in between
+    uint32_t* dkey_id = nullptr;
+    bool dkey_valid = false;
+    uint64_t particles_gen = 0, dkey_gen = 0;
+    pbf::DevParams dkey_P;
+    int dkey_g0[3] = {0, 0, 0};
+    uint32_t dkey_n[3] = {0, 0, 0};
     bool dense_window(int g0[3], uint32_t nd[3]) const;
     int ensure_dense();
     pbf::DenseArgs dense_args() const;

@@ -77,6 +77,12 @@ struct DenseArgs {
 // hash-sorted ids, re-deriving x* and v' as the predict pass does.
 void launch_d_keys_pred(const DevParams& P, const DenseArgs& D, const uint32_t* ids, const float4* pos,
                         const float4* vel, uint32_t* dkey, int sms, cudaStream_t st);
+// One scene: the predict pass writing the hash keys and, for each particle,
+// its predict-time window slot; the relabelling then gathers those slots.
+void launch_d_predict_hash(const DevParams& P, const DenseArgs& D, const float4* pos, const float4* vel,
+                           uint32_t* keys, uint32_t* dkey_id, int sms, cudaStream_t st);
+void launch_d_keys_gather(uint32_t n, const uint32_t* ids, const uint32_t* dkey_id, uint32_t* dkey, int sms,
+                          cudaStream_t st);
 void launch_d_permute(const DevParams& P, const uint32_t* order, const uint32_t* ids, const uint32_t* skeys,
                       const float4* pos, const float4* vel, float4* lx, float4* lxb, float4* lv, float4* lx0,
                       uint32_t* lid, uint32_t* lkey, uint32_t* inv, int sms, cudaStream_t st);
