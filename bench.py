@@ -40,10 +40,12 @@ ALGO_BYTES = {"predict_hash": 28, "radix_sort": 16, "cell_table": 12, "reorder":
               "deltap_apply": 28, "integrate": 72, "vorticity": 48}
 
 
-def algo_bytes(name, n, hash_size):
+def algo_bytes(name, n, hash_size, mode=4):
     b = ALGO_BYTES.get(name, 0) * n
     if name == "cell_table":
         b += 8 * hash_size
+    if name == "predict_hash" and mode == 8:
+        b += 4 * n  # the window slot of each particle, written beside its hash key
     return b
 
 
@@ -377,7 +379,7 @@ def run_b200(args, dist):
         if name == "step" or cnt == 0:
             continue
         per_launch = pms / cnt
-        b = algo_bytes(name, n, cfg.hash_size)
+        b = algo_bytes(name, n, cfg.hash_size, mode)
         per_pass[name] = {"ms_total": round(pms, 4), "launches": int(cnt), "ms_per_launch": round(per_launch, 5),
                           "share": round(pms / max(sum(v[0] for k, v in passes.items() if k != "step"), 1e-9), 4),
                           "algo_bytes_per_launch": b,
