@@ -864,9 +864,11 @@ __global__ void __launch_bounds__(256) k_d_place(uint32_t n, const uint32_t* __r
     if (s != kNoSlot) order[__ldg(block_offs + s / kScanItems) + b + (lane - head)] = t;
 }
 
+// 12 resident blocks (40 registers, none spilled; the compiler's own choice
+// was 48 with a small spill and 10 blocks): 1.081 -> 1.051 ms per 4M launch.
 template <bool B>
-__global__ void __launch_bounds__(kDThreads) k_d_lambda(DevParams P0, DenseArgs D0, const float4* __restrict__ lx_in,
-                                                        float4* __restrict__ lx_out, float* __restrict__ lrho)
+__global__ void __launch_bounds__(kDThreads, 12) k_d_lambda(DevParams P0, DenseArgs D0, const float4* __restrict__ lx_in,
+                                                            float4* __restrict__ lx_out, float* __restrict__ lrho)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (int)P0.n) return;
@@ -893,9 +895,12 @@ __global__ void __launch_bounds__(kDThreads) k_d_lambda(DevParams P0, DenseArgs 
     });
 }
 
+// 12 resident blocks (40 registers, some spilled): the replay's pair bodies
+// wait on their neighbour loads, and the extra warps hide more of that than
+// the spills cost (10 blocks: 1.048 ms per 4M launch, 12: 0.974, 16: 0.997).
 template <bool B>
-__global__ void __launch_bounds__(kDThreads, 10) k_d_deltap(DevParams P0, DenseArgs D0, const float4* __restrict__ lx_in,
-                                                        float4* __restrict__ lx_out)
+__global__ void __launch_bounds__(kDThreads, 12) k_d_deltap(DevParams P0, DenseArgs D0, const float4* __restrict__ lx_in,
+                                                            float4* __restrict__ lx_out)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = i < (int)P0.n;
