@@ -20,6 +20,11 @@
 namespace pbf {
 
 constexpr int kAThreads = 128;
+// The reverse pair passes and the recording Δp are held to 8 resident blocks
+// (at most 64 registers).  Left to itself the compiler gave the Δp adjoint 56
+// registers and 1.2 KB of spills; at 8 blocks the 16-scene backward of the C4
+// step takes 42.4 ms instead of 46.0 (10 or 12 blocks: 44.1 / 45.2 ms; 4: 49.5).
+constexpr int kAdjBlocks = 8;
 
 __device__ __forceinline__ float poly6_d(const DevParams& P, float r2)
 {
@@ -168,7 +173,7 @@ __global__ void __launch_bounds__(kAThreads) k_ad_lambda_rec(DevParams P, const 
     rhol[s] = rho;
 }
 
-__global__ void __launch_bounds__(kAThreads) k_ad_deltap_rec(DevParams P, const SceneDev* __restrict__ scenes,
+__global__ void __launch_bounds__(kAThreads, kAdjBlocks) k_ad_deltap_rec(DevParams P, const SceneDev* __restrict__ scenes,
                                                              const uint16_t* __restrict__ scene_of,
                                                              const uint32_t* __restrict__ order,
                                                              const int2* __restrict__ table,
@@ -245,7 +250,7 @@ __global__ void __launch_bounds__(kAThreads) k_ad_vorticity(DevParams P, const S
 // ---- CS_Integrate.glsl:135-280 reversed -------------------------------------------------------
 // (posb, velb) particle order (+ posb_s sorted, omb sorted when the vorticity
 // pass was reversed) -> gx (adjoint of x*), gv (of v'), x0b, tgrad.
-__global__ void __launch_bounds__(kAThreads) k_ad_integrate(
+__global__ void __launch_bounds__(kAThreads, kAdjBlocks) k_ad_integrate(
     DevParams P, const SceneDev* __restrict__ scenes, const uint16_t* __restrict__ scene_of,
     const uint32_t* __restrict__ order, const int2* __restrict__ table, const float4* __restrict__ xs,
     const float4* __restrict__ sv, const float4* __restrict__ cp_pos, const uint32_t* __restrict__ ids,
@@ -395,7 +400,7 @@ __global__ void __launch_bounds__(kAThreads) k_ad_integrate(
 // ---- CS_ComputeDeltaP.glsl:120-166 + CS_ApplyDeltaP.glsl:80-124 reversed --------------------
 // gin (adjoint of this iteration's output x*) -> gout.xyz (adjoint of the
 // input x*) and gout.w (adjoint of lambda), tgrad.
-__global__ void __launch_bounds__(kAThreads) k_ad_deltap(DevParams P, const SceneDev* __restrict__ scenes,
+__global__ void __launch_bounds__(kAThreads, kAdjBlocks) k_ad_deltap(DevParams P, const SceneDev* __restrict__ scenes,
                                                          const uint16_t* __restrict__ scene_of,
                                                          const uint32_t* __restrict__ order,
                                                          const int2* __restrict__ table,
@@ -463,7 +468,7 @@ __global__ void __launch_bounds__(kAThreads) k_ad_deltap(DevParams P, const Scen
 }
 
 // ---- CS_ComputeLambdas.glsl:108-162 reversed: gout.w (lambda adjoint) -> gout.xyz ---------------
-__global__ void __launch_bounds__(kAThreads) k_ad_lambda(DevParams P, const SceneDev* __restrict__ scenes,
+__global__ void __launch_bounds__(kAThreads, kAdjBlocks) k_ad_lambda(DevParams P, const SceneDev* __restrict__ scenes,
                                                          const uint16_t* __restrict__ scene_of,
                                                          const uint32_t* __restrict__ order,
                                                          const int2* __restrict__ table,
