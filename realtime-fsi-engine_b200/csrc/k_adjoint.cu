@@ -22,8 +22,9 @@ namespace pbf {
 constexpr int kAThreads = 128;
 // The reverse pair passes and the recording Δp are held to 8 resident blocks
 // (at most 64 registers).  Left to itself the compiler gave the Δp adjoint 56
-// registers and 1.2 KB of spills; at 8 blocks the 16-scene backward of the C4
-// step takes 42.4 ms instead of 46.0 (10 or 12 blocks: 44.1 / 45.2 ms; 4: 49.5).
+// registers and 1.2 KB of spills; at 8 blocks the backward of one step (16
+// substeps x 4 iterations) of 16 scenes of 32,768 particles takes 42.4 ms
+// instead of 46.0 (10 or 12 blocks: 44.1 / 45.2 ms; 4: 49.5).
 constexpr int kAdjBlocks = 8;
 
 __device__ __forceinline__ float poly6_d(const DevParams& P, float r2)
