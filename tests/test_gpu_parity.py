@@ -371,6 +371,35 @@ def test_dense_runs_agree_with_bucket_walk(have_gpu):
     assert np.array_equal(b["pos"], d["pos"]) and np.array_equal(b["vel"], d["vel"])
 
 
+def test_dense_window_change_and_particle_upload_between_steps(have_gpu):
+    """In mode 8 the predict pass also writes each particle's window slot,
+    which the relabelling of the same substep gathers.  Moving the walls (a
+    new window) and uploading new particle state between steps make the
+    relabelling derive the slots again; over a run with both, mode 8 stays
+    bit-identical to mode 4."""
+    cfg, pos, vel = scenes.c0(16, seed=4)
+    cfg.particle_count = len(pos)
+    out = []
+    for mode in (4, 8):
+        fl = P.PBFluids(cfg)
+        fl.set_option(1, mode)
+        fl.setParticles(P.make_particles(pos, vel))
+        for _ in range(2):
+            fl.step()
+        hi = list(cfg.bounds_max)
+        fl.setBounds(list(cfg.bounds_min), [hi[0] * 0.9, hi[1], hi[2] * 1.1], cfg.bound_damping)
+        for _ in range(2):
+            fl.step()
+        mid = fl.readbackParticles()
+        mid["pos"][:, 1] += np.float32(0.25 * cfg.h)
+        fl.uploadParticles(mid)
+        for _ in range(2):
+            fl.step()
+        out.append(fl.readbackParticles())
+    assert np.isfinite(out[1]["pos"]).all()
+    assert np.array_equal(out[0]["pos"], out[1]["pos"]) and np.array_equal(out[0]["vel"], out[1]["vel"])
+
+
 @pytest.mark.parametrize("hash_size", [64, 4096])
 def test_dense_runs_fall_back_on_hash_collisions(have_gpu, hash_size):
     """A small hash table makes neighbouring cells share buckets, which the
