@@ -27,19 +27,25 @@
 // and fail r <= h.  Within a run the cells come x - 1, x, x + 1, the
 // reference's innermost loop.
 //
-// (a) and (b) depend only on the window and the hash mask: one flag per slot,
-// computed when either changes, as is, per cell, the distance to the nearest
-// other cell of its bucket.  For (c), every pass that moves particles checks
-// each particle now more than 0.9 h from its predict-time position: unless
-// that distance shows no colliding cell can be in a query's neighbourhood
-// (settle_drift), it marks the window cells within 1.01 h of where the
-// particle is whose neighbourhood holds a colliding cell ("dirty" for the rest
-// of the substep): only a query in such a cell can see it through another
-// cell's bucket.  A particle whose cell fails (a), (b) or (c) walks the 27
-// hashed buckets (through the hash-slot -> label map).  Both walks test
-// candidates in chunks into a hit mask and run the shared pair bodies of
-// masked_body.cuh for the hits in candidate order, so a pair's arithmetic is
-// the same in every walk and every mode.
+// (b) and (c) hold or fail row by row: the argument above is about the three
+// buckets of one row (dz, dy) at a time.  (a) and (b) depend only on the
+// window and the hash mask: one 9-bit mask of failing rows per slot, computed
+// when either changes, as is, per cell, the distance to the nearest other
+// cell of its bucket.  For (c), every pass that moves particles checks each
+// particle now more than 0.9 h from its predict-time position: unless that
+// distance shows no colliding cell can be in a query's neighbourhood
+// (settle_drift), it marks, in the window cells within 1.01 h of where the
+// particle is whose neighbourhood holds a colliding cell, the row of that
+// cell ("dirty" for the rest of the substep): only a query in such a cell can
+// see it, and only through that row's buckets.  A particle walks the runs of
+// its clean rows and the hashed buckets (through the hash-slot -> label map)
+// of the others, in the reference's row order; outside the window interior
+// all 27 buckets.  The walks test candidates in chunks into a hit mask and
+// run the shared pair bodies of masked_body.cuh for the hits in candidate
+// order, so a pair's arithmetic is the same in every walk and every mode.
+// The near-zero corner of a box meets exact 32-bit collisions of the hash
+// (cells (1, -1, z) and (-1, 1, z) share every bucket), so the cells along
+// its three edges there always have some rows on the buckets.
 //
 // Work saved on top of the runs:
 //   * passes after the first iteration take their threads in current-cell
@@ -63,6 +69,8 @@
 namespace pbf {
 
 constexpr int kDThreads = 128;
+// The nine rows (dz, dy) of a cell's neighbourhood, bit (dz + 1) * 3 + (dy + 1).
+constexpr uint32_t kAllRows = 0x1FFu;
 
 // Batches (B = true): the scene k of a label, hash-sorted index or slot
 // replaces the hash mask, walls, SDF and window of P and D with its own, so
@@ -221,9 +229,12 @@ __device__ __forceinline__ uint32_t window_of_slot(DenseArgs& D, uint32_t& mask,
     return g - D.slot0;
 }
 
-// Conditions (a) and (b) per window slot.
+// Conditions (a) and (b) per window slot, (b) per row: bit (dz+1)*3+(dy+1)
+// is set when a neighbour cell N of that row shares its bucket with a cell
+// M != N within Chebyshev distance 2; 0x1FF when the cell is at the window's
+// edge (a).
 template <bool B>
-__global__ void __launch_bounds__(128) k_d_clean(DenseArgs D0, uint32_t mask0, uint8_t* __restrict__ clean,
+__global__ void __launch_bounds__(128) k_d_clean(DenseArgs D0, uint32_t mask0, uint16_t* __restrict__ clean,
                                                  uint32_t* __restrict__ unclean)
 {
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -232,14 +243,14 @@ __global__ void __launch_bounds__(128) k_d_clean(DenseArgs D0, uint32_t mask0, u
         uint32_t mask = mask0;
         const uint32_t s = window_of_slot<B>(D, mask, g);
         const uint32_t lx = s % D.nx, ly = (s / D.nx) % D.ny, lz = s / (D.nx * D.ny);
-        uint8_t ok = 0;
+        uint32_t bad = kAllRows;
         if (lx >= 1 && lx + 1 < D.nx && ly >= 1 && ly + 1 < D.ny && lz >= 1 && lz + 1 < D.nz) {
             const int cx = D.gx0 + (int)lx, cy = D.gy0 + (int)ly, cz = D.gz0 + (int)lz;
             uint32_t hn[27];
 #pragma unroll
             for (int u = 0; u < 27; ++u)
                 hn[u] = grid_hash(cx + u % 3 - 1, cy + (u / 3) % 3 - 1, cz + u / 9 - 1, mask);
-            bool good = true;
+            bad = 0;
 #pragma unroll 1
             for (int m = 0; m < 125; ++m) {
                 const int mx = m % 5 - 2, my = (m / 5) % 5 - 2, mz = m / 25 - 2;
@@ -247,12 +258,12 @@ __global__ void __launch_bounds__(128) k_d_clean(DenseArgs D0, uint32_t mask0, u
                 const bool inner = mx >= -1 && mx <= 1 && my >= -1 && my <= 1 && mz >= -1 && mz <= 1;
                 const int self_u = inner ? (mz + 1) * 9 + (my + 1) * 3 + (mx + 1) : -1;
 #pragma unroll
-                for (int u = 0; u < 27; ++u) good &= !(hm == hn[u] && u != self_u);
+                for (int u = 0; u < 27; ++u)
+                    if (hm == hn[u] && u != self_u) bad |= 1u << (u / 3);
             }
-            ok = good ? 1 : 0;
-            if (!good) atomicAdd(unclean, 1u);
+            if (bad) atomicAdd(unclean, 1u);
         }
-        clean[g] = ok;
+        clean[g] = (uint16_t)bad;
     }
 }
 
@@ -534,14 +545,24 @@ struct RunWalkList {
     }
 };
 
-// The 27 hashed buckets in label space, in the reference's order.
-struct BucketWalkLabels {
+
+// The 27 cells row by row in the reference's order: a row whose bit is set in
+// `rows` walks its three hashed buckets (through the hash-slot -> label map),
+// the others their x-run of labels.  A row's run holds the pairs of its
+// buckets in the same order when (b) and (c) hold for that row, so the walk
+// visits exactly the pairs of the bucket walk whatever the mask; rows =
+// kAllRows is the bucket walk itself (s0 is not read then).
+struct MixedWalk {
     const DevParams& P;
+    const int2* __restrict__ runs;
     const int2* __restrict__ htable;
     const uint32_t* __restrict__ inv;
     const float4* __restrict__ X;
     float4 xi;
     int self;
+    int s0;
+    int nx, nxy;
+    uint32_t rows;
     template <class Hit, class Body>
     __device__ __forceinline__ void operator()(Hit&& hit, Body&& body) const
     {
@@ -551,12 +572,17 @@ struct BucketWalkLabels {
             const uint32_t hz = (uint32_t)(cz + dz) * kP3;
 #pragma unroll 1
             for (int dy = -1; dy <= 1; ++dy) {
-                const uint32_t hyz = hz ^ ((uint32_t)(cy + dy) * kP2);
+                if ((rows >> ((dz + 1) * 3 + (dy + 1))) & 1u) {
+                    const uint32_t hyz = hz ^ ((uint32_t)(cy + dy) * kP2);
 #pragma unroll 1
-                for (int dx = -1; dx <= 1; ++dx) {
-                    const int2 se = __ldg(htable + ((((uint32_t)(cx + dx) * kP1) ^ hyz) & P.mask));
-                    if (se.x == -1) continue;
-                    masked_range<kChunk>(X, xi, self, se.x, se.y, InvMap{inv}, hit, body);
+                    for (int dx = -1; dx <= 1; ++dx) {
+                        const int2 se = __ldg(htable + ((((uint32_t)(cx + dx) * kP1) ^ hyz) & P.mask));
+                        if (se.x == -1) continue;
+                        masked_range<kChunk>(X, xi, self, se.x, se.y, InvMap{inv}, hit, body);
+                    }
+                } else {
+                    const int2 r = __ldg(runs + s0 + dz * nxy + dy * nx);
+                    label_range<kRunChunk>(X, xi, self, r.x, r.y, hit, body);
                 }
             }
         }
@@ -564,7 +590,8 @@ struct BucketWalkLabels {
 };
 
 // Window slot of the particle's current cell when its neighbourhood lies in
-// the window interior (else -1); fast_slot adds (b) and (c).
+// the window interior (else -1); dense_rows adds the rows that (b) and (c)
+// send to the buckets.
 __device__ __forceinline__ int interior_slot(const DevParams& P, const DenseArgs& D, float4 xi)
 {
     const uint32_t ux = (uint32_t)cell_coord(xi.x, P.h) - (uint32_t)D.gx0;
@@ -575,10 +602,19 @@ __device__ __forceinline__ int interior_slot(const DevParams& P, const DenseArgs
     return -1;
 }
 
-__device__ __forceinline__ int fast_slot(const DevParams& P, const DenseArgs& D, float4 xi)
+// The interior slot (or -1) and in `rows` the rows that walk their buckets:
+// those (b) or (c) rules out for runs, all of them outside the interior.
+__device__ __forceinline__ int dense_rows(const DevParams& P, const DenseArgs& D, float4 xi, uint32_t& rows)
 {
     const int s0 = interior_slot(P, D, xi);
-    return (s0 >= 0 && __ldg(D.clean + s0) && !D.dirty[s0]) ? s0 : -1;
+    rows = s0 >= 0 ? (uint32_t)__ldg(D.clean + s0) | D.dirty[s0] : kAllRows;
+    return s0;
+}
+
+__device__ __forceinline__ MixedWalk mixed_walk(const DevParams& P, const DenseArgs& D, const float4* X, float4 xi,
+                                                int t, int s0, uint32_t rows)
+{
+    return MixedWalk{P, D.runs, D.htable, D.inv, X, xi, t, s0, (int)D.nx, (int)(D.nx * D.ny), rows};
 }
 
 __device__ __forceinline__ void count_bucket_walk(const DenseArgs& D)
@@ -587,19 +623,20 @@ __device__ __forceinline__ void count_bucket_walk(const DenseArgs& D)
     if ((threadIdx.x & 31u) == (uint32_t)(__ffs(am) - 1)) atomicAdd(D.flag + 1, (uint32_t)__popc(am));
 }
 
-// Run core(walker) with the run walk when (a), (b) and (c) hold, else with
-// the bucket walk.
+// Run core(walker) with the run walk when (a), (b) and (c) hold for every
+// row, else with the mixed walk (the rows they rule out through the buckets).
 template <class Core>
 __device__ __forceinline__ void with_dense_walker(const DevParams& P, const DenseArgs& D, const float4* X, float4 xi,
                                                   int t, Core&& core)
 {
-    const int s0 = fast_slot(P, D, xi);
-    if (s0 >= 0) {
+    uint32_t rows;
+    const int s0 = dense_rows(P, D, xi, rows);
+    if (rows == 0) {
         core(RunWalk{D.runs, X, xi, t, s0, (int)D.nx, (int)(D.nx * D.ny)});
         return;
     }
     count_bucket_walk(D);
-    core(BucketWalkLabels{P, D.htable, D.inv, X, xi, t});
+    core(mixed_walk(P, D, X, xi, t, s0, rows));
 }
 
 // A particle at x, predict-time position xb, that has moved more than the
@@ -610,10 +647,11 @@ __device__ __forceinline__ void with_dense_walker(const DevParams& P, const Dens
 // neighbour cells within 3, so within 3 + cheb(cell(x), M) of M.  When M's
 // nearest same-bucket cell is farther (dcol), the particle is harmless;
 // otherwise every such N near the reach is found and the query cells within
-// reach that hold N, but not M, in their neighbourhood are marked dirty (a
-// query holding both has a collision in its neighbourhood and walks the
-// buckets anyway).  Kept out of line: it takes no registers from the passes.
-__device__ __noinline__ void settle_drift(const uint8_t* dcol, uint8_t* dirty, uint32_t* count, float h, uint32_t mask,
+// reach that hold N, but not M, in their neighbourhood get the bit of N's row
+// (dz, dy) set in their dirty mask (a query holding both has a collision in
+// its neighbourhood, and (b) already sends both rows to the buckets).  Kept
+// out of line: it takes no registers from the passes.
+__device__ __noinline__ void settle_drift(const uint8_t* dcol, uint32_t* dirty, uint32_t* count, float h, uint32_t mask,
                                           float x, float y, float z, float bx, float by, float bz, int gx0, int gy0,
                                           int gz0, uint32_t nx, uint32_t ny, uint32_t nz)
 {
@@ -656,7 +694,8 @@ __device__ __noinline__ void settle_drift(const uint8_t* dcol, uint8_t* dirty, u
                             if (dm <= 1) continue;
                             const uint32_t ux = (uint32_t)cx - (uint32_t)g0[0], uy = (uint32_t)cy - (uint32_t)g0[1],
                                            uz = (uint32_t)cz - (uint32_t)g0[2];
-                            if (ux < nx && uy < ny && uz < nz) dirty[(uz * ny + uy) * nx + ux] = 1;
+                            if (ux < nx && uy < ny && uz < nz)
+                                atomicOr(dirty + (uz * ny + uy) * nx + ux, 1u << (int)((qz - cz + 1) * 3 + (qy - cy + 1)));
                             marked = true;
                         }
             }
@@ -878,8 +917,9 @@ __global__ void __launch_bounds__(kDThreads, 12) k_d_lambda(DevParams P0, DenseA
         float rho, den;
         float3 g;
         float4 out;
-        const int s0 = fast_slot(P, D, xi);
-        if (s0 >= 0) {
+        uint32_t rows;
+        const int s0 = dense_rows(P, D, xi, rows);
+        if (rows == 0) {
             int q = 0;
             out = lambda_core(P, GSrc{lx_in}, xi,
                               RunWalkRec{D.runs, lx_in, xi, t, s0, (int)D.nx, (int)(D.nx * D.ny), D.hm, P.n, &q}, rho, g,
@@ -887,7 +927,7 @@ __global__ void __launch_bounds__(kDThreads, 12) k_d_lambda(DevParams P0, DenseA
             D.hcnt[t] = q <= kListChunks ? (uint8_t)q : kNoList;
         } else {
             count_bucket_walk(D);
-            out = lambda_core(P, GSrc{lx_in}, xi, BucketWalkLabels{P, D.htable, D.inv, lx_in, xi, t}, rho, g, den);
+            out = lambda_core(P, GSrc{lx_in}, xi, mixed_walk(P, D, lx_in, xi, t, s0, rows), rho, g, den);
             D.hcnt[t] = kNoList;
         }
         lx_out[t] = out;
@@ -951,14 +991,15 @@ __global__ void __launch_bounds__(kDThreads, 10) k_d_integrate(DevParams P0, Den
                 // x* unless the walls or the SDF moved the particle: record
                 // the hit masks, and where a particle moved, mark the query
                 // cells whose runs hold it
-                const int s0 = fast_slot(P, D, x4);
-                if (s0 >= 0) {
+                uint32_t rows;
+                const int s0 = dense_rows(P, D, x4, rows);
+                if (rows == 0) {
                     int q = 0;
                     core(RunWalkRec{D.runs, lx, x4, t, s0, (int)D.nx, (int)(D.nx * D.ny), D.hm, P.n, &q});
                     D.hcnt[t] = q <= kListChunks ? (uint8_t)q : kNoList;
                 } else {
                     count_bucket_walk(D);
-                    core(BucketWalkLabels{P, D.htable, D.inv, lx, x4, t});
+                    core(mixed_walk(P, D, lx, x4, t, s0, rows));
                     D.hcnt[t] = kNoList;
                 }
                 if (xo.x != x4.x || xo.y != x4.y || xo.z != x4.z) {
@@ -1053,7 +1094,7 @@ void launch_d_permute(const DevParams& P, const uint32_t* order, const uint32_t*
                                                                lkey, inv);
 }
 
-void launch_d_clean(const DenseArgs& D, uint32_t mask, uint8_t* clean, uint32_t* unclean, int sms, cudaStream_t st)
+void launch_d_clean(const DenseArgs& D, uint32_t mask, uint16_t* clean, uint32_t* unclean, int sms, cudaStream_t st)
 {
     PBF_DENSE_LAUNCH(k_d_clean, capped_grid(D.total, 128, sms, 16), 128, D, mask, clean, unclean);
 }

@@ -381,7 +381,7 @@ int pbf_batch::dense_step_body()
         BCK(cudaMemsetAsync(dtable, 0xFF, sizeof(int2) * (size_t)T, stream));
         launch_build_table(n, msorted, dtable, sms, stream);
         launch_d_runs(D, dtable, druns, sms, stream);
-        BCK(cudaMemsetAsync(ddirty, 0, (size_t)T, stream));
+        BCK(cudaMemsetAsync(ddirty, 0, sizeof(uint32_t) * (size_t)T, stream));
         BCK(cudaMemsetAsync(dflag, 0, sizeof(uint32_t), stream));
         launches += 3;
         for (uint32_t it = 1; it <= iters; ++it) {

@@ -161,7 +161,9 @@ struct pbf_batch {
     float* lrho = nullptr;
     uint32_t *lid = nullptr, *lkey = nullptr, *inv = nullptr;
     int2 *dtable = nullptr, *druns = nullptr;
-    uint8_t *dclean = nullptr, *ddcol = nullptr, *ddirty = nullptr, *dhcnt = nullptr, *dvmark = nullptr;
+    uint16_t* dclean = nullptr;
+    uint32_t* ddirty = nullptr;
+    uint8_t *ddcol = nullptr, *dhcnt = nullptr, *dvmark = nullptr;
     uint16_t* dslot_scene = nullptr;
     uint32_t *dflag = nullptr, *dslot = nullptr, *dord = nullptr, *dcnt = nullptr, *dbsum = nullptr;
     uint32_t* dhm = nullptr;

@@ -676,7 +676,7 @@ int pbf_handle::stage(int st, uint32_t iter)
             launch_build_table(n, msorted, dtable, sms, stream);
             launch_d_runs(dense_args(), dtable, druns, sms, stream);
             launches += 2;
-            CK(cudaMemsetAsync(ddirty, 0, slots, stream));
+            CK(cudaMemsetAsync(ddirty, 0, sizeof(uint32_t) * slots, stream));
             dord_iter = 0;
             dlist_iter = 0;
             dvlist_ready = false;

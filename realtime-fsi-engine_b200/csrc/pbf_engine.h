@@ -56,9 +56,9 @@ struct pbf_handle {
     // mode 8: runs of a dense cell window
     int2* dtable = nullptr;      // per window slot: label range
     int2* druns = nullptr;       // per window slot: label range of its x-run (slots s-1 .. s+1)
-    uint8_t* dclean = nullptr;   // per window slot: no hash collision near the cell
+    uint16_t* dclean = nullptr;  // per window slot: rows whose buckets a hash collision near the cell affects
     uint8_t* ddcol = nullptr;    // per window slot: distance to the nearest other cell of its bucket
-    uint8_t* ddirty = nullptr;   // per window slot: a moved particle within reach (per substep)
+    uint32_t* ddirty = nullptr;  // per window slot: rows through which a moved particle is within reach (per substep)
     uint32_t* dflag = nullptr;   // [0] drift-bound crossings, [1] bucket walks, [2] unclean slots
     // thread order of the passes after particles have moved (labels by current cell)
     uint32_t *dslot = nullptr, *dord = nullptr, *dcnt = nullptr, *dbsum = nullptr;

@@ -57,9 +57,11 @@ struct DenseArgs {
     uint8_t* vmark;        // per window slot: a query there sees a particle integrate moved (no replay)
     uint32_t* rec_slot;    // delta-p / integrate (may be null): current slot of each output position
     uint32_t* rec_cnt;     //   and per-slot counts (zeroed by the caller), for the next pass's order
-    const uint8_t* clean;  // per window slot: 1 = no hash collision near the cell
+    const uint16_t* clean; // per window slot: rows (bit (dz+1)*3+(dy+1)) whose buckets a hash collision near the cell
+                           //   affects; 0 = none, 0x1FF at the window's edge
     const uint8_t* dcol;   // per window slot: Chebyshev distance to the nearest other cell of its bucket
-    uint8_t* dirty;        // per window slot: a moved particle with a colliding cell near is within reach
+    uint32_t* dirty;       // per window slot: rows through whose buckets a moved particle with a colliding cell near
+                           //   is within reach (same bits as `clean`)
     const int2* htable;    // the hashed cell table (sorted slots)
     const uint32_t* inv;   // hash slot -> label
     const float4* xb;      // predict-time x*, label order
@@ -86,7 +88,7 @@ void launch_d_keys_gather(uint32_t n, const uint32_t* ids, const uint32_t* dkey_
 void launch_d_permute(const DevParams& P, const uint32_t* order, const uint32_t* ids, const uint32_t* skeys,
                       const float4* pos, const float4* vel, float4* lx, float4* lxb, float4* lv, float4* lx0,
                       uint32_t* lid, uint32_t* lkey, uint32_t* inv, int sms, cudaStream_t st);
-void launch_d_clean(const DenseArgs& D, uint32_t mask, uint8_t* clean, uint32_t* unclean, int sms, cudaStream_t st);
+void launch_d_clean(const DenseArgs& D, uint32_t mask, uint16_t* clean, uint32_t* unclean, int sms, cudaStream_t st);
 void launch_d_dcol(const DenseArgs& D, uint32_t mask, uint8_t* dcol, int sms, cudaStream_t st);
 void launch_d_runs(const DenseArgs& D, const int2* cells, int2* runs, int sms, cudaStream_t st);
 // Labels bucketed by the window slot of their current cell (X) into order[n].
