@@ -134,6 +134,17 @@ __device__ __forceinline__ uint32_t dense_key(const DenseArgs& D, int cx, int cy
            (wrap_axis(cz, D.gz0, D.nz) * D.ny + wrap_axis(cy, D.gy0, D.ny)) * D.nx + wrap_axis(cx, D.gx0, D.nx);
 }
 
+// One scene's relabelling key of a cell: its window slot, or D.total (the
+// overflow slot, after every window slot) for a cell outside the window.
+// Runs never reach the overflow slot's labels; the bucket walk reaches them
+// through the hash-slot -> label map like any other.
+__device__ __forceinline__ uint32_t scene_key(const DenseArgs& D, int cx, int cy, int cz)
+{
+    const uint32_t ux = (uint32_t)cx - (uint32_t)D.gx0, uy = (uint32_t)cy - (uint32_t)D.gy0,
+                   uz = (uint32_t)cz - (uint32_t)D.gz0;
+    return (ux < D.nx && uy < D.ny && uz < D.nz) ? (uz * D.ny + uy) * D.nx + ux : D.total;
+}
+
 // Window slot of each hash-sorted particle's predict-time cell, x* re-derived
 // from (pos, vel) of particle ids[s] exactly as the predict pass derives it.
 template <bool B>
@@ -147,7 +158,8 @@ __global__ void __launch_bounds__(256) k_d_keys_pred(DevParams P0, DenseArgs D0,
         float3 vp, xs;
         predict_particle(P0, __ldg(pos + id), __ldg(vel + id), vp, xs);
         with_scene<B>(P0, D0, (int)s, [&](const DevParams& P, const DenseArgs& D) {
-            dkey[s] = dense_key(D, cell_coord(xs.x, P.h), cell_coord(xs.y, P.h), cell_coord(xs.z, P.h));
+            const int cx = cell_coord(xs.x, P.h), cy = cell_coord(xs.y, P.h), cz = cell_coord(xs.z, P.h);
+            dkey[s] = B ? dense_key(D, cx, cy, cz) : scene_key(D, cx, cy, cz);
         });
     }
 }
@@ -166,7 +178,7 @@ __global__ void __launch_bounds__(256) k_d_predict_hash(DevParams P, DenseArgs D
         predict_particle(P, __ldg(pos + i), __ldg(vel + i), vp, xs);
         const int cx = cell_coord(xs.x, P.h), cy = cell_coord(xs.y, P.h), cz = cell_coord(xs.z, P.h);
         keys[i] = grid_hash(cx, cy, cz, P.mask);
-        dkey_id[i] = dense_key(D, cx, cy, cz);
+        dkey_id[i] = scene_key(D, cx, cy, cz);
     }
 }
 
@@ -903,6 +915,50 @@ __global__ void __launch_bounds__(256) k_d_place(uint32_t n, const uint32_t* __r
     if (s != kNoSlot) order[__ldg(block_offs + s / kScanItems) + b + (lane - head)] = t;
 }
 
+// ---- relabelling of one scene by counting -----------------------------------------------
+// Labels in the order of a stable sort of the hash-sorted sequence by slot
+// key, without the sort: within the window a cell has one hash, so all its
+// particles lie in one bucket's range of the hash sort, in id order, and a
+// particle's label is the start of its slot (a counting scan over the slots)
+// plus the number of particles of the same slot before it in that range.
+// The overflow slot's particles (cells outside the window, from several
+// buckets) are placed in any order: runs never reach them, and everything
+// else they take part in follows the hash-sorted order through `inv`.
+__global__ void __launch_bounds__(256) k_d_relabel_count(uint32_t n, const uint32_t* __restrict__ dkey,
+                                                         uint32_t* __restrict__ cnt)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t k = s < n ? __ldg(dkey + s) : kNoSlot;
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t head, len;
+    slot_run(k, lane, head, len);
+    if (lane == head && k != kNoSlot) atomicAdd(cnt + k, len);
+}
+
+__global__ void __launch_bounds__(256) k_d_relabel_place(uint32_t n, const uint32_t* __restrict__ dkey,
+                                                         const uint32_t* __restrict__ skeys,
+                                                         const uint32_t* __restrict__ start,
+                                                         const uint32_t* __restrict__ block_offs, uint32_t overflow,
+                                                         uint32_t* __restrict__ overflow_count,
+                                                         uint32_t* __restrict__ order, uint32_t* __restrict__ sorted_keys)
+{
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += stride) {
+        const uint32_t k = __ldg(dkey + s);
+        uint32_t r = 0;
+        if (k == overflow) {
+            r = atomicAdd(overflow_count, 1u);
+        } else {
+            // earlier particles of this slot in this bucket's range
+            const uint32_t hk = __ldg(skeys + s);
+            for (uint32_t q = s; q > 0 && __ldg(skeys + q - 1) == hk; --q) r += __ldg(dkey + q - 1) == k ? 1u : 0u;
+        }
+        const uint32_t t = __ldg(block_offs + k / kScanItems) + __ldg(start + k) + r;
+        order[t] = s;
+        sorted_keys[t] = k;
+    }
+}
+
 // 12 resident blocks (40 registers, none spilled; the compiler's own choice
 // was 48 with a small spill and 10 blocks): 1.081 -> 1.051 ms per 4M launch.
 template <bool B>
@@ -1122,6 +1178,22 @@ void launch_d_order(const DevParams& P, const DenseArgs& D, const float4* X, uin
     k_d_scan_blocks<<<nb, 1024, 0, st>>>(cnt, m, block_sums);
     k_d_scan_sums<<<1, 1024, 0, st>>>(block_sums, nb);
     k_d_place<<<g, 256, 0, st>>>(P.n, slot_of, cnt, block_sums, order);
+    *launches += 4;
+}
+
+void launch_d_relabel(uint32_t n, uint32_t slots, const uint32_t* dkey, const uint32_t* skeys, uint32_t* cnt,
+                      uint32_t* block_sums, uint32_t* overflow_count, uint32_t* order, uint32_t* sorted_keys, int sms,
+                      cudaStream_t st, uint64_t* launches)
+{
+    const uint32_t m = slots + 1u;  // window slots + the overflow slot
+    const uint32_t nb = order_scan_blocks(slots);
+    cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * m, st);
+    cudaMemsetAsync(overflow_count, 0, sizeof(uint32_t), st);
+    k_d_relabel_count<<<(n + 255u) / 256u, 256, 0, st>>>(n, dkey, cnt);
+    k_d_scan_blocks<<<nb, 1024, 0, st>>>(cnt, m, block_sums);
+    k_d_scan_sums<<<1, 1024, 0, st>>>(block_sums, nb);
+    k_d_relabel_place<<<capped_grid(n, 256, sms, 8), 256, 0, st>>>(n, dkey, skeys, cnt, block_sums, slots,
+                                                                  overflow_count, order, sorted_keys);
     *launches += 4;
 }
 

@@ -492,7 +492,7 @@ int pbf_handle::ensure_dense()
     if (same) return PBF_OK;
     if (capturing) return set_error(PBF_ERR_INVALID, "dense cell window changed during graph capture");
     if (slots > cap_slots || !dtable) {
-        if ((rc = dalloc(dtable, slots)) || (rc = dalloc(druns, slots)) || (rc = dalloc(dcnt, slots + 1)) ||
+        if ((rc = dalloc(dtable, slots + 1)) || (rc = dalloc(druns, slots)) || (rc = dalloc(dcnt, slots + 1)) ||
             (rc = dalloc(dbsum, order_scan_blocks((uint32_t)slots))) || (rc = dalloc(dclean, slots)) ||
             (rc = dalloc(ddcol, slots)) ||
             (rc = dalloc(ddirty, slots)) || (rc = dalloc(dvmark, slots)))
@@ -666,13 +666,15 @@ int pbf_handle::stage(int st, uint32_t iter)
                 launch_d_keys_pred(P, D, ids, pos, vel, mcode, sms, stream);
             ++launches;
             const uint64_t slots = (uint64_t)dwin_n[0] * dwin_n[1] * dwin_n[2];
-            uint32_t bits = 1;
-            while ((1ull << bits) < slots) ++bits;
-            uint32_t* msorted = nullptr;
-            launch_radix_sort(n, bits, mcode, mka, mia, mkb, mib, hist, totals, &msorted, &order, stream, &launches);
+            // labels by counting (launch_d_relabel), into the relabelling's sort buffers
+            uint32_t* msorted = mka;
+            order = mia;
+            launch_d_relabel(n, (uint32_t)slots, mcode, skeys, dcnt, dbsum, dflag + 3, order, msorted, sms, stream,
+                             &launches);
             launch_d_permute(P, order, ids, skeys, pos, vel, lx[0], lxb, lv, lx0, lid, lkey, inv, sms, stream);
             ++launches;
-            CK(cudaMemsetAsync(dtable, 0xFF, sizeof(int2) * slots, stream));
+            // (slot `slots` holds the overflow's labels)
+            CK(cudaMemsetAsync(dtable, 0xFF, sizeof(int2) * (slots + 1), stream));
             launch_build_table(n, msorted, dtable, sms, stream);
             launch_d_runs(dense_args(), dtable, druns, sms, stream);
             launches += 2;

@@ -59,7 +59,7 @@ struct pbf_handle {
     uint16_t* dclean = nullptr;  // per window slot: rows whose buckets a hash collision near the cell affects
     uint8_t* ddcol = nullptr;    // per window slot: distance to the nearest other cell of its bucket
     uint32_t* ddirty = nullptr;  // per window slot: rows through which a moved particle is within reach (per substep)
-    uint32_t* dflag = nullptr;   // [0] drift-bound crossings, [1] bucket walks, [2] unclean slots
+    uint32_t* dflag = nullptr;   // [0] drift-bound crossings, [1] bucket walks, [2] unclean slots, [3] overflow labels
     // thread order of the passes after particles have moved (labels by current cell)
     uint32_t *dslot = nullptr, *dord = nullptr, *dcnt = nullptr, *dbsum = nullptr;
     uint32_t cap_ord_n = 0;

@@ -96,6 +96,14 @@ void launch_d_runs(const DenseArgs& D, const int2* cells, int2* runs, int sms, c
 uint32_t order_scan_blocks(uint32_t slots);
 void launch_d_order(const DevParams& P, const DenseArgs& D, const float4* X, uint32_t* slot_of, uint32_t* cnt,
                     uint32_t* block_sums, uint32_t* order, cudaStream_t st, uint64_t* launches);
+// One scene's relabelling: for the hash-sorted sequence of slot keys dkey[n]
+// (window slots, `slots` for the overflow) with hash keys skeys[n], order[t]
+// = hash-sorted index of label t and sorted_keys[t] its key, as a stable sort
+// by key orders them (the overflow slot's entries in any order).  Scratch:
+// cnt[slots + 1], block_sums[order_scan_blocks(slots)], one overflow counter.
+void launch_d_relabel(uint32_t n, uint32_t slots, const uint32_t* dkey, const uint32_t* skeys, uint32_t* cnt,
+                      uint32_t* block_sums, uint32_t* overflow_count, uint32_t* order, uint32_t* sorted_keys, int sms,
+                      cudaStream_t st, uint64_t* launches);
 // The same order from slots and counts a pass recorded (DenseArgs::rec_slot / rec_cnt).
 void launch_d_order_recorded(const DevParams& P, const DenseArgs& D, const uint32_t* slot_of, uint32_t* cnt,
                              uint32_t* block_sums, uint32_t* order, cudaStream_t st, uint64_t* launches);

@@ -400,6 +400,31 @@ def test_dense_window_change_and_particle_upload_between_steps(have_gpu):
     assert np.array_equal(out[0]["pos"], out[1]["pos"]) and np.array_equal(out[0]["vel"], out[1]["vel"])
 
 
+def test_dense_particles_predicted_outside_the_window(have_gpu):
+    """A particle whose predict-time cell lies outside the dense window (its
+    velocity carries x* more than the window's margin past a wall) is
+    relabelled into the overflow slot after every window slot; runs never
+    reach it and the bucket walk finds it through the hash sort.  Over steps
+    with many such particles, mode 8 stays bit-identical to mode 4."""
+    cfg, pos, vel = scenes.c0(16, seed=5)
+    cfg.particle_count = len(pos)
+    vel = np.array(vel, dtype=np.float32, copy=True)
+    rng = np.random.default_rng(5)
+    pick = rng.choice(len(pos), 300, replace=False)
+    # 40 m/s over a 1/120 s substep is 8 cells of h = 0.04, beyond the 6-cell margin
+    vel[pick, :3] = rng.normal(0.0, 40.0, (len(pick), 3)).astype(np.float32)
+    out = []
+    for mode in (4, 8):
+        fl = P.PBFluids(cfg)
+        fl.set_option(1, mode)
+        fl.setParticles(P.make_particles(pos, vel))
+        for _ in range(3):
+            fl.step()
+        out.append(fl.readbackParticles())
+    assert np.isfinite(out[1]["pos"]).all()
+    assert np.array_equal(out[0]["pos"], out[1]["pos"]) and np.array_equal(out[0]["vel"], out[1]["vel"])
+
+
 @pytest.mark.parametrize("hash_size", [64, 4096])
 def test_dense_runs_fall_back_on_hash_collisions(have_gpu, hash_size):
     """A small hash table makes neighbouring cells share buckets, which the
