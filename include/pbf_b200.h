@@ -318,11 +318,12 @@ int pbf_set_use_graph(pbf_handle* h, int on);
 #define PBF_OPT_SPATIAL_ORDER 1
 int pbf_set_option(pbf_handle* h, int option, int value);
 
-/* Mode 8 statistics: particle passes that walked the hashed buckets (since
- * the window was set up), particles beyond the 0.9 h drift bound that marked
- * the cells within their reach in the last substep (a same-bucket cell was
- * near; counted per pass), and window cells whose neighbourhood has a hash
- * collision.  Zeros in mode 4. */
+/* Mode 8 statistics: particle passes that walked some rows of their
+ * neighbourhood through the hashed buckets (since the window was set up),
+ * particles beyond the 0.9 h drift bound that marked the cells within their
+ * reach in the last substep (a same-bucket cell was near; counted per pass),
+ * and window cells whose neighbourhood has a hash collision.  Zeros in
+ * mode 4. */
 int pbf_list_stats(pbf_handle* h, uint32_t* full_walks, uint32_t* bucket_walks, uint32_t* marked_buckets);
 
 /* ---- health ------------------------------------------------------------- */

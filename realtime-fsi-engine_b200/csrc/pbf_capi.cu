@@ -1321,8 +1321,8 @@ extern "C" int pbf_list_stats(pbf_handle* h, uint32_t* full_walks, uint32_t* buc
     if (!full_walks || !bucket_walks || !marked_buckets) return set_error(PBF_ERR_INVALID, "null argument");
     *full_walks = *bucket_walks = *marked_buckets = 0;
     if (h->effective_mode() == 8) {
-        // mode 8: particle passes that walked the hashed buckets since the
-        // window was set up, particles of the last substep that moved beyond
+        // mode 8: particle passes that walked some rows through the hashed
+        // buckets since the window was set up, particles of the last substep that moved beyond
         // the drift bound near a colliding cell and marked cells (counted per
         // pass), window cells that fail the collision test
         if (h->dflag) {
