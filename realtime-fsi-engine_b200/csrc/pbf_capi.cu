@@ -666,11 +666,22 @@ int pbf_handle::stage(int st, uint32_t iter)
                 launch_d_keys_pred(P, D, ids, pos, vel, mcode, sms, stream);
             ++launches;
             const uint64_t slots = (uint64_t)dwin_n[0] * dwin_n[1] * dwin_n[2];
-            // labels by counting (launch_d_relabel), into the relabelling's sort buffers
             uint32_t* msorted = mka;
-            order = mia;
-            launch_d_relabel(n, (uint32_t)slots, mcode, skeys, dcnt, dbsum, dflag + 3, order, msorted, sms, stream,
-                             &launches);
+            if ((uint64_t)derived.hash_size * 64u >= n) {
+                // labels by counting (launch_d_relabel), into the relabelling's sort
+                // buffers; each particle scans the part of its bucket before it, so
+                // the buckets must stay short
+                order = mia;
+                launch_d_relabel(n, (uint32_t)slots, mcode, skeys, dcnt, dbsum, dflag + 3, order, msorted, sms,
+                                 stream, &launches);
+            } else {
+                // a hash table far smaller than the particle count: a stable radix
+                // sort of the keys (the overflow key `slots` included)
+                uint32_t bits = 1;
+                while ((1ull << bits) <= slots) ++bits;
+                launch_radix_sort(n, bits, mcode, mka, mia, mkb, mib, hist, totals, &msorted, &order, stream,
+                                  &launches);
+            }
             launch_d_permute(P, order, ids, skeys, pos, vel, lx[0], lxb, lv, lx0, lid, lkey, inv, sms, stream);
             ++launches;
             // (slot `slots` holds the overflow's labels)

@@ -425,12 +425,13 @@ def test_dense_particles_predicted_outside_the_window(have_gpu):
     assert np.array_equal(out[0]["pos"], out[1]["pos"]) and np.array_equal(out[0]["vel"], out[1]["vel"])
 
 
-@pytest.mark.parametrize("hash_size", [64, 4096])
+@pytest.mark.parametrize("hash_size", [32, 64, 4096])
 def test_dense_runs_fall_back_on_hash_collisions(have_gpu, hash_size):
     """A small hash table makes neighbouring cells share buckets, which the
-    reference then walks twice: cells with such a collision within two cells
-    walk the hashed buckets (64: all of them; 4096: some): bit-identical to
-    mode 4."""
+    reference then walks twice: the rows with such a collision within two
+    cells walk the hashed buckets (32, 64: nearly all of them; 4096: some):
+    bit-identical to mode 4.  With 32 buckets for 4,096 particles the window
+    relabelling takes the radix sort instead of counting."""
     cfg, pos, vel = scenes.c0(16, seed=2)
     cfg.particle_count = len(pos)
     cfg.hash_size = hash_size
