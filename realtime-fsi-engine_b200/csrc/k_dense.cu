@@ -4,8 +4,9 @@
 // The scene's box plus a margin of cells on each side is a dense window.
 // After the hash sort of a substep, every particle is relabelled by the
 // window slot of its predict-time cell (z, then y, then x; cells outside the
-// window wrap into it) and the per-particle arrays are gathered into that
-// label order.  The three x-adjacent cells of a row are then one contiguous
+// window go to one overflow slot after it for one scene, wrap into the
+// scene's window in a batch) and the per-particle arrays are gathered into
+// that label order.  The three x-adjacent cells of a row are then one contiguous
 // label range, so a particle walks 9 runs of about 24 candidates instead of
 // 27 buckets of about 8 (the reference, CS_ComputeLambdas.glsl:126-150).
 //
@@ -23,8 +24,8 @@
 // is more than 2h - 0.9h from c's box, so out of range; by (b) no other
 // colliding cell is nearer.  So the in-range candidates of bucket hash(N) are
 // N's own, in id order (the stable sort), and the run walk sees N's particles
-// in the same order; particles of other cells wrapped into N's slot are far
-// and fail r <= h.  Within a run the cells come x - 1, x, x + 1, the
+// in the same order; particles of other cells wrapped into N's slot (a
+// batch) are far and fail r <= h.  Within a run the cells come x - 1, x, x + 1, the
 // reference's innermost loop.
 //
 // (b) and (c) hold or fail row by row: the argument above is about the three
