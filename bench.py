@@ -254,6 +254,35 @@ def cpu_reference_rate(budget_s, sample=(64, 64, 64), max_steps=50, warmup=0):
                       "host threads"}, cfg
 
 
+def neighbour_work(pos, h, step_ms, passes, sample=100000, seed=0):
+    """Neighbour work per step at a particle state (a host-side count after the timed
+    runs, not timed): the candidates a query tests (the particles of the 27 cells
+    around its own, the reference's bucket walk when no buckets collide) and the
+    in-range pairs (r <= h, self excluded; a seeded sample of queries), per particle,
+    and both per second over the `passes` neighbour passes of a step."""
+    try:
+        from scipy.ndimage import uniform_filter
+        from scipy.spatial import cKDTree
+    except ImportError:
+        return None
+    x = np.asarray(pos, np.float64)[:, :3]
+    c = np.floor(x / h).astype(np.int64)
+    c -= c.min(axis=0) - 1
+    dims = c.max(axis=0) + 2
+    occ = np.zeros((dims[2], dims[1], dims[0]), np.float64)
+    np.add.at(occ, (c[:, 2], c[:, 1], c[:, 0]), 1.0)
+    box = np.rint(uniform_filter(occ, size=3, mode="constant") * 27.0)
+    cand = float((occ * box).sum() / len(x))
+    rng = np.random.default_rng(seed)
+    q = x[rng.choice(len(x), min(sample, len(x)), replace=False)]
+    pairs = float(np.mean(cKDTree(x).query_ball_point(q, h, return_length=True)) - 1.0)
+    per_s = len(x) * passes / (step_ms / 1e3)
+    return {"candidates_per_particle": round(cand, 1), "in_range_pairs_per_particle": round(pairs, 2),
+            "neighbour_passes_per_step": passes, "candidate_tests_per_s": cand * per_s,
+            "pair_evaluations_per_s": pairs * per_s,
+            "counted": f"on the state after the timed steps; pairs from {len(q)} seeded queries (k-d tree, r <= h)"}
+
+
 def c2_config(desc, cfg, n):
     """The workload's config object, identical in both arms."""
     return {"workload": desc, "particles_per_gpu": n, "substeps": int(cfg.substep_iterations),
@@ -369,6 +398,9 @@ def run_b200(args, dist):
     e2e_s = dist.max(time.perf_counter() - t0)
     e2e = {"value": n * subs * args.e2e_steps * dist.world / e2e_s, "unit": METRIC,
            "h2d_bytes_per_step": n * 48, "d2h_bytes_per_step": n * 48}
+    # lambda and delta-p per iteration and integrate per substep, vorticity once per step
+    nb_passes = (2 * cfg.solver_iterations + 1) * subs + (1 if cfg.enable_vorticity else 0)
+    work = neighbour_work(host["pos"], cfg.h, ms_max / args.steps, nb_passes) if dist.rank == 0 else None
 
     # roofline of the dominant kernel (largest share of device time)
     pk = peaks()
@@ -403,7 +435,7 @@ def run_b200(args, dist):
             "config": c2_config(desc, cfg, n), "neighbour_mode": mode,
             "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU",
             "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
-            "passes": per_pass, "nonfinite_particles": int(bad), "impl": "b200"}
+            "passes": per_pass, "neighbour_work": work, "nonfinite_particles": int(bad), "impl": "b200"}
     if ws1 is not None:
         # pbf_list_stats before and after the timed steps (bucket walks, drift marks, unclean cells)
         line["walk_stats"] = {"before": list(ws0), "after": list(ws1)}
