@@ -232,7 +232,9 @@ enum pbf_stage {
     PBF_STAGE_TABLE = 3,     /* CS_BuildOffsets: clear + build the hash-cell table  */
     PBF_STAGE_REORDER = 4,   /* gather x*, v', x into sorted float4 SoA (+ LOD)     */
     PBF_STAGE_LAMBDA = 5,    /* CS_ComputeLambdas (iteration `iter`, 1-based)       */
-    PBF_STAGE_DELTAP = 6,    /* CS_ComputeDeltaP + CS_ApplyDeltaP fused             */
+    PBF_STAGE_DELTAP = 6,    /* CS_ComputeDeltaP + CS_ApplyDeltaP fused; reads the  */
+                             /* per-particle sums PBF_STAGE_LAMBDA of the same      */
+                             /* iteration wrote, so it runs after that stage        */
     PBF_STAGE_INTEGRATE = 7, /* CS_Integrate                                         */
     PBF_STAGE_VORTICITY = 8  /* CS_VorticityConfinement pass 1                       */
 };

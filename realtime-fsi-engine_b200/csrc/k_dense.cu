@@ -960,10 +960,12 @@ __global__ void __launch_bounds__(256) k_d_relabel_place(uint32_t n, const uint3
     }
 }
 
-// 12 resident blocks (40 registers, none spilled; the compiler's own choice
-// was 48 with a small spill and 10 blocks): 1.081 -> 1.051 ms per 4M launch.
+// 10 resident blocks (48 registers, 8 bytes spilled): with the s_corr sum of
+// the delta-p pass in its pair body, 12 blocks (40 registers, 132 bytes
+// spilled) took 1.225 ms per 4M launch against 1.165.  The pass also writes
+// each particle's lambda-independent delta-p part (DevParams::dpb).
 template <bool B>
-__global__ void __launch_bounds__(kDThreads, 12) k_d_lambda(DevParams P0, DenseArgs D0, const float4* __restrict__ lx_in,
+__global__ void __launch_bounds__(kDThreads, 10) k_d_lambda(DevParams P0, DenseArgs D0, const float4* __restrict__ lx_in,
                                                             float4* __restrict__ lx_out, float* __restrict__ lrho)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -976,27 +978,30 @@ __global__ void __launch_bounds__(kDThreads, 12) k_d_lambda(DevParams P0, DenseA
         float4 out;
         uint32_t rows;
         const int s0 = dense_rows(P, D, xi, rows);
+        float3 b;
         if (rows == 0) {
             int q = 0;
             out = lambda_core(P, GSrc{lx_in}, xi,
                               RunWalkRec{D.runs, lx_in, xi, t, s0, (int)D.nx, (int)(D.nx * D.ny), D.hm, P.n, &q}, rho, g,
-                              den);
+                              den, b);
             D.hcnt[t] = q <= kListChunks ? (uint8_t)q : kNoList;
         } else {
             count_bucket_walk(D);
-            out = lambda_core(P, GSrc{lx_in}, xi, mixed_walk(P, D, lx_in, xi, t, s0, rows), rho, g, den);
+            out = lambda_core(P, GSrc{lx_in}, xi, mixed_walk(P, D, lx_in, xi, t, s0, rows), rho, g, den, b);
             D.hcnt[t] = kNoList;
         }
         lx_out[t] = out;
         lrho[t] = rho;
+        P.dpb[t] = make_float4(b.x, b.y, b.z, 0.f);
     });
 }
 
-// 12 resident blocks (40 registers, some spilled): the replay's pair bodies
-// wait on their neighbour loads, and the extra warps hide more of that than
-// the spills cost (10 blocks: 1.048 ms per 4M launch, 12: 0.974, 16: 0.997).
+// 16 resident blocks (32 registers, spills on the SDF projection's path): the
+// replay's pair bodies, which load and scale only lambda_j, wait on their
+// neighbour loads, and the extra warps hide more of that than the spills cost
+// (12 blocks: 0.758 ms per 4M launch, 16: 0.731).
 template <bool B>
-__global__ void __launch_bounds__(kDThreads, 12) k_d_deltap(DevParams P0, DenseArgs D0, const float4* __restrict__ lx_in,
+__global__ void __launch_bounds__(kDThreads, 16) k_d_deltap(DevParams P0, DenseArgs D0, const float4* __restrict__ lx_in,
                                                             float4* __restrict__ lx_out)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1006,15 +1011,18 @@ __global__ void __launch_bounds__(kDThreads, 12) k_d_deltap(DevParams P0, DenseA
         float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
         if (live) {
             const float4 xi = __ldg(lx_in + t);
+            const float4 b4 = __ldg(P.dpb + t);
+            const float3 b = make_float3(b4.x, b4.y, b4.z);
             float3 dp;
             if (D.use_list && __ldg(D.hcnt + t) != kNoList) {
                 // the lambda pass of this iteration walked this particle's runs
                 const int s0 = interior_slot(P, D, xi);
                 out = deltap_core(P, P.sdf, GSrc{lx_in}, xi,
-                                  RunWalkList{D.runs, lx_in, xi, t, s0, (int)D.nx, (int)(D.nx * D.ny), D.hm, P.n}, dp);
+                                  RunWalkList{D.runs, lx_in, xi, t, s0, (int)D.nx, (int)(D.nx * D.ny), D.hm, P.n}, dp,
+                                  b);
             } else {
                 with_dense_walker(P, D, lx_in, xi, t,
-                                  [&](auto&& walk) { out = deltap_core(P, P.sdf, GSrc{lx_in}, xi, walk, dp); });
+                                  [&](auto&& walk) { out = deltap_core(P, P.sdf, GSrc{lx_in}, xi, walk, dp, b); });
             }
             lx_out[t] = out;
             check_drift(P, D, out, t);

@@ -104,14 +104,21 @@ struct HashWalk {
 
 // ---- CS_ComputeLambdas.glsl:108-162 -----------------------------------------------------------
 // Returns (x*, lambda); also rho, grad C_i (the scaled sum of spiky
-// gradients) and the denominator sum |grad C|^2 + eps that lambda divides by
-// (the adjoint replays them).
+// gradients), the denominator sum |grad C|^2 + eps that lambda divides by
+// (the adjoint replays them) and, in b_out, the part of the delta-p sum of
+// CS_ComputeDeltaP.glsl:120-166 that does not depend on the neighbours'
+// lambdas: lambda_i * sum_j gradW_ij + sum_j s_corr(r_ij) * gradW_ij (before
+// the 1/rho0 scale).  The delta-p pass of the same iteration, over the same
+// positions and pairs, then adds only sum_j lambda_j * gradW_ij.
 template <class XS, class Walk>
 __device__ __forceinline__ float4 lambda_core(const DevParams& P, XS X, float4 xi, Walk&& walk, float& rho_out,
-                                              float3& g_out, float& den_out)
+                                              float3& g_out, float& den_out, float3& b_out)
 {
-    float rho = P.w0_self, sg = 0.f, gz = 0.f;
-    float2 gxy = make_float2(0.f, 0.f);
+    // s_corr = -k (W / W(dq))^n per pair: the pair body sums (W / W(dq))^n *
+    // gradW, the factor -k is applied once after the walk
+    const bool scorr = P.scorr && P.wq > 1e-12f;
+    float rho = P.w0_self, sg = 0.f, gz = 0.f, sz = 0.f;
+    float2 gxy = make_float2(0.f, 0.f), sxy = make_float2(0.f, 0.f);
     const float2 xyi = make_float2(xi.x, xi.y);
     walk([&](float r2) { return r2 <= P.h2; },
          [&](int k) {
@@ -119,26 +126,44 @@ __device__ __forceinline__ float4 lambda_core(const DevParams& P, XS X, float4 x
              const float2 rxy = sub_f32x2(xyi, make_float2(xj.x, xj.y));
              const float rx = rxy.x, ry = rxy.y, rz = xi.z - xj.z;
              const float r2 = rx * rx + ry * ry + rz * rz;
-             rho += poly6_in(P, r2);
+             const float w = poly6_in(P, r2);
+             rho += w;
              if (r2 >= 1e-10f) {
                  const float sc = spiky_scale(P, r2);
                  const float2 axy = mul_f32x2(rxy, sc);
                  const float ax = axy.x, ay = axy.y, az = rz * sc;
-                 sg += (ax * ax + ay * ay + az * az) * P.inv_rho0_sq;
+                 sg += ax * ax + ay * ay + az * az;
                  gxy = add_f32x2(gxy, axy);
                  gz += az;
+                 if (scorr) {
+                     const float ratio = w * P.inv_wq;
+                     float pw;
+                     if (P.ncorr_is4) {
+                         const float q = ratio * ratio;
+                         pw = q * q;
+                     } else {
+                         pw = powf(ratio, P.n_corr);
+                     }
+                     sxy = fma_f32x2(axy, pw, sxy);
+                     sz = __fmaf_rn(az, pw, sz);
+                 }
              }
          });
+    const float lam_gx = gxy.x, lam_gy = gxy.y, lam_gz = gz;  // sum_j gradW_ij, unscaled
     float gx = gxy.x, gy = gxy.y;
     gx *= P.inv_rho0;
     gy *= P.inv_rho0;
     gz *= P.inv_rho0;
     const float C = fmaxf(rho / P.rho0 - 1.0f, -P.cohesion);
-    sg += gx * gx + gy * gy + gz * gz;
+    sg = sg * P.inv_rho0_sq + (gx * gx + gy * gy + gz * gz);
     rho_out = rho;
     g_out = make_float3(gx, gy, gz);
     den_out = sg + P.eps;
-    return make_float4(xi.x, xi.y, xi.z, -C / den_out);
+    const float lam = -C / den_out;
+    const float kc = scorr ? -P.k_corr : 0.f;
+    b_out = make_float3(__fmaf_rn(lam, lam_gx, kc * sxy.x), __fmaf_rn(lam, lam_gy, kc * sxy.y),
+                        __fmaf_rn(lam, lam_gz, kc * sz));
+    return make_float4(xi.x, xi.y, xi.z, lam);
 }
 
 __device__ __forceinline__ float4 lambda_particle_x(const DevParams& P, const int2* __restrict__ table,
@@ -146,7 +171,10 @@ __device__ __forceinline__ float4 lambda_particle_x(const DevParams& P, const in
                                                     float& rho_out, float3& g_out, float& den_out)
 {
     const float4 xi = __ldg(xin + s);
-    return lambda_core(P, GSrc{xin}, xi, HashWalk{P, table, mask, xin, xi, s}, rho_out, g_out, den_out);
+    float3 b;
+    const float4 out = lambda_core(P, GSrc{xin}, xi, HashWalk{P, table, mask, xin, xi, s}, rho_out, g_out, den_out, b);
+    P.dpb[s] = make_float4(b.x, b.y, b.z, 0.f);
+    return out;
 }
 
 __device__ __forceinline__ float4 lambda_particle(const DevParams& P, const int2* __restrict__ table, uint32_t mask,
@@ -158,7 +186,8 @@ __device__ __forceinline__ float4 lambda_particle(const DevParams& P, const int2
 }
 
 // s_corr * (poly6 coefficient form) of CS_ComputeDeltaP.glsl:94-104 added to
-// lambda_i + lambda_j; valid for r2 < h2.
+// lambda_i + lambda_j; valid for r2 < h2 (the adjoint's reverse delta-p pass
+// differentiates it per pair).
 __device__ __forceinline__ float scorr_term(const DevParams& P, float r2)
 {
     const float d = P.h2 - r2;
@@ -178,14 +207,17 @@ __device__ __forceinline__ float scorr_term(const DevParams& P, float r2)
 }
 
 // ---- CS_ComputeDeltaP.glsl:120-166 + CS_ApplyDeltaP.glsl:80-124 --------------------------------
-// Returns (x* + dp, lambda); dp_raw = dp before the 0.5 h clamp.
+// Returns (x* + dp, lambda); dp_raw = dp before the 0.5 h clamp.  b is the
+// lambda pass's b_out for this particle: the shader's per-pair factor
+// (lambda_i + lambda_j + s_corr) * gradW_ij is summed as b + sum_j lambda_j *
+// gradW_ij, so the pair body here loads and scales only lambda_j.
 template <class XS, class Walk>
 __device__ __forceinline__ float4 deltap_core(const DevParams& P, const SdfDev& sdf, XS X, float4 xi, Walk&& walk,
-                                              float3& dp_raw)
+                                              float3& dp_raw, float3 b)
 {
     const float li = xi.w;
-    float dz = 0.f;
-    float2 dxy = make_float2(0.f, 0.f);
+    float dz = b.z;
+    float2 dxy = make_float2(b.x, b.y);
     const float2 xyi = make_float2(xi.x, xi.y);
     walk([&](float r2) { return r2 <= P.h2 && r2 >= 1e-10f; },
          [&](int k) {
@@ -193,10 +225,7 @@ __device__ __forceinline__ float4 deltap_core(const DevParams& P, const SdfDev& 
              const float2 rxy = sub_f32x2(xyi, make_float2(xj.x, xj.y));
              const float rx = rxy.x, ry = rxy.y, rz = xi.z - xj.z;
              const float r2 = rx * rx + ry * ry + rz * rz;
-             const float sc = spiky_scale(P, r2);
-             float f = li + xj.w;
-             if (P.scorr) f += scorr_term(P, r2);
-             const float g = sc * f;
+             const float g = spiky_scale(P, r2) * xj.w;
              dxy = fma_f32x2(rxy, g, dxy);
              dz = __fmaf_rn(rz, g, dz);
          });
@@ -226,7 +255,9 @@ __device__ __forceinline__ float4 deltap_particle_x(const DevParams& P, const in
                                                     const float4* __restrict__ xin, int s, float3& dp_raw)
 {
     const float4 xi = __ldg(xin + s);
-    return deltap_core(P, sdf, GSrc{xin}, xi, HashWalk{P, table, mask, xin, xi, s}, dp_raw);
+    const float4 b = __ldg(P.dpb + s);
+    return deltap_core(P, sdf, GSrc{xin}, xi, HashWalk{P, table, mask, xin, xi, s}, dp_raw,
+                       make_float3(b.x, b.y, b.z));
 }
 
 __device__ __forceinline__ float4 deltap_particle(const DevParams& P, const int2* __restrict__ table, uint32_t mask,

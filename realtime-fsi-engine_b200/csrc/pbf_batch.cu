@@ -76,7 +76,7 @@ pbf_batch::~pbf_batch()
     bfree(pos); bfree(vel); bfree(pred); bfree(aos); bfree(scene_of); bfree(scenes_dev);
     bfree(keys); bfree(ka); bfree(ia); bfree(kb); bfree(ib); bfree(hist); bfree(totals); bfree(table);
     bfree(mcode); bfree(mka); bfree(mia); bfree(mkb); bfree(mib);
-    bfree(sx[0]); bfree(sx[1]); bfree(sv); bfree(sx0); bfree(somega); bfree(rho); bfree(lod);
+    bfree(sx[0]); bfree(sx[1]); bfree(sv); bfree(sx0); bfree(somega); bfree(dpb); bfree(rho); bfree(lod);
     bfree(save_pos); bfree(save_vel);
     dense_free();
     ad_free();
@@ -141,6 +141,7 @@ DevParams pbf_batch::dev_params() const
     P.lod_max_dist = derived.lod_max_dist;
     P.min_lod = derived.min_lod;
     P.max_lod = derived.max_lod;
+    P.dpb = dpb;
     return P;
 }
 
@@ -540,7 +541,7 @@ extern "C" int pbf_batch_create(const pbf_fluid_config* cfg, const pbf_scene_des
         (rc = balloc(b->mcode, c)) || (rc = balloc(b->mka, c)) || (rc = balloc(b->mia, c)) ||
         (rc = balloc(b->mkb, c)) || (rc = balloc(b->mib, c)) || (rc = balloc(b->sx[0], c)) ||
         (rc = balloc(b->sx[1], c)) || (rc = balloc(b->sv, c)) || (rc = balloc(b->sx0, c)) ||
-        (rc = balloc(b->somega, c)) || (rc = balloc(b->rho, c)) || (rc = balloc(b->lod, c))) {
+        (rc = balloc(b->somega, c)) || (rc = balloc(b->dpb, c)) || (rc = balloc(b->rho, c)) || (rc = balloc(b->lod, c))) {
         delete b;
         return rc;
     }

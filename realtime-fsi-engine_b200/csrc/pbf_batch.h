@@ -139,6 +139,7 @@ struct pbf_batch {
     uint32_t* order = nullptr;
     // sorted order
     float4 *sx[2] = {nullptr, nullptr}, *sv = nullptr, *sx0 = nullptr, *somega = nullptr;
+    float4* dpb = nullptr;  // lambda-independent part of each delta-p sum (DevParams::dpb)
     float* rho = nullptr;
     uint32_t* lod = nullptr;
     // autotuner state snapshot

@@ -242,6 +242,7 @@ DevParams pbf_handle::dev_params() const
     P.min_lod = derived.min_lod;
     P.max_lod = derived.max_lod;
     P.sdf = sdf_dev();
+    P.dpb = dpb;
     return P;
 }
 
@@ -275,7 +276,7 @@ int pbf_handle::ensure_capacity(uint32_t need_n)
         if ((rc = dalloc(pos, c)) || (rc = dalloc(vel, c)) || (rc = dalloc(pred, c)) || (rc = dalloc(aos, 3 * c)) ||
             (rc = dalloc(keys, c)) || (rc = dalloc(ka, c)) || (rc = dalloc(mcode, c)) || (rc = dalloc(mka, c)) ||
             (rc = dalloc(mia, c)) || (rc = dalloc(mkb, c)) || (rc = dalloc(mib, c)) || (rc = dalloc(ia, c)) || (rc = dalloc(kb, c)) || (rc = dalloc(ib, c)) || (rc = dalloc(sx[0], c)) ||
-            (rc = dalloc(sx[1], c)) || (rc = dalloc(sv, c)) || (rc = dalloc(sx0, c)) || (rc = dalloc(somega, c)) ||
+            (rc = dalloc(sx[1], c)) || (rc = dalloc(sv, c)) || (rc = dalloc(sx0, c)) || (rc = dalloc(somega, c)) || (rc = dalloc(dpb, c)) ||
             (rc = dalloc(rho, c)) || (rc = dalloc(lod, c)) || (rc = dalloc(cand, 2 * c)) ||
             (rc = dalloc(ct_counts, (size_t)contact_num_blocks(need_n) + 1)))
             return rc;
@@ -311,7 +312,7 @@ pbf_handle::~pbf_handle()
     for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
     dfree(pos); dfree(vel); dfree(pred); dfree(aos); dfree(keys);
     dfree(mcode); dfree(mka); dfree(mia); dfree(mkb); dfree(mib); dfree(ka); dfree(ia); dfree(kb); dfree(ib);
-    dfree(sx[0]); dfree(sx[1]); dfree(sv); dfree(sx0); dfree(somega); dfree(rho); dfree(lod);
+    dfree(sx[0]); dfree(sx[1]); dfree(sv); dfree(sx0); dfree(somega); dfree(dpb); dfree(rho); dfree(lod);
     dfree(hist); dfree(totals); dfree(table); dfree(cand); dfree(ct_counts); dfree(scalars);
     dfree(lx[0]); dfree(lx[1]); dfree(lxb); dfree(lv); dfree(lx0); dfree(lom); dfree(lrho);
     dfree(lid); dfree(lkey); dfree(inv); dfree(dkey_id);

@@ -98,6 +98,7 @@ struct pbf_handle {
     float4* sv = nullptr;
     float4* sx0 = nullptr;
     float4* somega = nullptr;
+    float4* dpb = nullptr;     // lambda-independent part of each delta-p sum (DevParams::dpb)
     float* rho = nullptr;
     uint32_t* lod = nullptr;
     // contacts

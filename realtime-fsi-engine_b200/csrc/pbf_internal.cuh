@@ -67,6 +67,10 @@ struct DevParams {
     float lod_max_dist;
     uint32_t min_lod, max_lod;
     SdfDev sdf;
+    // per particle, indexed as the position arrays of the solver iterations:
+    // the lambda-independent part of the delta-p sum, written by each lambda
+    // pass and read by the delta-p pass of the same iteration (masked_body.cuh)
+    float4* dpb;
 };
 
 __device__ __forceinline__ uint32_t grid_hash(int cx, int cy, int cz, uint32_t mask)
