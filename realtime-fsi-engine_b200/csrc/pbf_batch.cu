@@ -549,6 +549,7 @@ extern "C" int pbf_batch_create(const pbf_fluid_config* cfg, const pbf_scene_des
     cudaMemsetAsync(b->vel, 0, sizeof(float4) * c, b->stream);
     cudaMemsetAsync(b->pred, 0, sizeof(float4) * c, b->stream);
     cudaMemsetAsync(b->somega, 0, sizeof(float4) * c, b->stream);
+    cudaMemsetAsync(b->dpb, 0, sizeof(float4) * c, b->stream);
     if (total) cudaMemcpyAsync(b->scene_of, sid.data(), sizeof(uint16_t) * total, cudaMemcpyHostToDevice, b->stream);
     if ((rc = b->upload_scenes())) {
         delete b;

@@ -927,6 +927,8 @@ extern "C" int pbf_set_particles(pbf_handle* h, const pbf_particle* ps, uint32_t
     launch_unpack_particles(n, h->aos, h->pos, h->pred, h->vel, h->num_sms, h->stream);
     ++h->launches;
     CK(cudaMemsetAsync(h->somega, 0, sizeof(float4) * n, h->stream));
+    // a delta-p stage run without the lambda stage before it reads zeros, not stale memory
+    CK(cudaMemsetAsync(h->dpb, 0, sizeof(float4) * n, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     return PBF_OK;
 }
@@ -983,6 +985,7 @@ extern "C" int pbf_set_particles_device(pbf_handle* h, const void* pos4, const v
             int rc = h->ensure_capacity(n);
             if (rc) return rc;
             CK(cudaMemsetAsync(h->pred, 0, sizeof(float4) * n, h->stream));
+            CK(cudaMemsetAsync(h->dpb, 0, sizeof(float4) * n, h->stream));
         }
     }
     if (n == 0) return PBF_OK;
