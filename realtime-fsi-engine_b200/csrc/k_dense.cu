@@ -1046,10 +1046,10 @@ __global__ void __launch_bounds__(kDThreads, 10) k_d_integrate(DevParams P0, Den
         if (live) {
             const float4 x4 = __ldg(lx + t);
             const float4 v0 = __ldg(lv + t);
-            const float4 p0 = lx0[t];
             float4 vo, om;
             auto core = [&](auto&& walk) {
-                integrate_core(P, P.bmin, P.bmax, P.sdf, GSrc{lx}, GSrc{lv}, x4, v0, p0, walk, xo, vo, om);
+                integrate_core(P, P.bmin, P.bmax, P.sdf, GSrc{lx}, GSrc{lv}, x4, v0, [&] { return lx0[t]; }, walk, xo,
+                               vo, om);
             };
             if constexpr (R) {
                 // the vorticity pass walks the committed positions, equal to
@@ -1099,7 +1099,9 @@ __global__ void __launch_bounds__(kDThreads, 12) k_d_vorticity(DevParams P0, Den
         const float4 xi = __ldg(lx0 + t);
         float3 dv;
         bool any = false;
-        auto core = [&](auto&& walk) { any = vorticity_core(P, GSrc{lx0}, GMagX{lx0}, xi, __ldg(lom + t), walk, dv); };
+        auto core = [&](auto&& walk) {
+            any = vorticity_core(P, GSrc{lx0}, GMagX{lx0}, xi, [&] { return __ldg(lom + t); }, walk, dv);
+        };
         const int s0 = D.use_list && __ldg(D.hcnt + t) != kNoList ? interior_slot(P, D, xi) : -1;
         if (s0 >= 0 && !D.vmark[s0])
             // integrate walked this particle's runs over the same positions

@@ -271,9 +271,9 @@ __device__ __forceinline__ float4 deltap_particle(const DevParams& P, const int2
 // From x* (x4), the predicted velocity v0, the substep start p0 and the
 // neighbours' (X, V): the committed position xo (w = p0.w), velocity vo
 // (w = v0.w) and, when vorticity is on, omega4 = (omega, |omega|).
-template <class XS, class VS, class Walk>
+template <class XS, class VS, class P0, class Walk>
 __device__ __forceinline__ void integrate_core(const DevParams& P, const float* bmin, const float* bmax,
-                                               const SdfDev& sdf, XS X, VS V, float4 x4, float4 v0, float4 p0,
+                                               const SdfDev& sdf, XS X, VS V, float4 x4, float4 v0, P0&& p0_load,
                                                Walk&& walk, float4& xo, float4& vo, float4& omega4)
 {
     float fz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
@@ -306,6 +306,9 @@ __device__ __forceinline__ void integrate_core(const DevParams& P, const float* 
                  }
              });
     }
+    // the substep-start position is needed only now: loaded after the walk,
+    // it holds no registers across it
+    const float4 p0 = p0_load();
     const float fx = fxy.x, fy = fxy.y;
     float3 x = make_float3(x4.x, x4.y, x4.z);
     float vdx = 0.f, vdy = 0.f, vdz = 0.f;
@@ -362,10 +365,9 @@ __device__ __forceinline__ void integrate_particle(const DevParams& P, const int
 {
     const float4 x4 = __ldg(xs + s);
     const float4 v0 = __ldg(sv + s);
-    const float4 p0 = sx0[s];
     float4 xo, vo, om;
-    integrate_core(P, bmin, bmax, sdf, GSrc{xs}, GSrc{sv}, x4, v0, p0, HashWalk{P, table, mask, xs, x4, s}, xo, vo,
-                   om);
+    integrate_core(P, bmin, bmax, sdf, GSrc{xs}, GSrc{sv}, x4, v0, [&] { return sx0[s]; },
+                   HashWalk{P, table, mask, xs, x4, s}, xo, vo, om);
     if (P.vort_on) somega[s] = om;
     const uint32_t id = __ldg(ids + s);
     pos[id] = xo;
@@ -377,8 +379,8 @@ __device__ __forceinline__ void integrate_particle(const DevParams& P, const int
 // Velocity increment eps (N x omega_i) dt of a particle at xi with vorticity
 // w; returns false when |eta| < 1e-6 (no change).
 // MS: source of the neighbours' |omega| (MS[k] -> float).
-template <class XS, class MS, class Walk>
-__device__ __forceinline__ bool vorticity_core(const DevParams& P, XS X, MS OMAG, float4 xi, float4 w, Walk&& walk,
+template <class XS, class MS, class WL, class Walk>
+__device__ __forceinline__ bool vorticity_core(const DevParams& P, XS X, MS OMAG, float4 xi, WL&& w_load, Walk&& walk,
                                                float3& dv)
 {
     float ez = 0.f;
@@ -400,6 +402,7 @@ __device__ __forceinline__ bool vorticity_core(const DevParams& P, XS X, MS OMAG
     ez *= P.inv_rho0;
     const float el = sqrtf(ex * ex + ey * ey + ez * ez);
     if (el < 1e-6f) return false;
+    const float4 w = w_load();  // the particle's own omega, loaded after the walk
     const float nx = ex / el, ny = ey / el, nz = ez / el;
     const float crx = __fmaf_rn(ny, w.z, -__fmul_rn(nz, w.y)), cry = __fmaf_rn(nz, w.x, -__fmul_rn(nx, w.z)),
                 crz = __fmaf_rn(nx, w.y, -__fmul_rn(ny, w.x));
@@ -417,7 +420,8 @@ __device__ __forceinline__ void vorticity_particle(const DevParams& P, const int
 {
     const float4 xi = __ldg(spos + s);
     float3 dv;
-    if (!vorticity_core(P, GSrc{spos}, GMag{somega}, xi, __ldg(somega + s), HashWalk{P, table, mask, spos, xi, s}, dv))
+    if (!vorticity_core(P, GSrc{spos}, GMag{somega}, xi, [&] { return __ldg(somega + s); },
+                        HashWalk{P, table, mask, spos, xi, s}, dv))
         return;
     const uint32_t id = __ldg(ids + s);
     float4 v = vel[id];

@@ -83,10 +83,26 @@ def test_cell_table_bit_exact(have_gpu):
         assert (t[:, 1] - t[:, 0])[t[:, 0] >= 0].sum() == n
 
 
+# A fixture with one config field overridden ("file.npz:field=value"): the
+# s_corr exponent other than 4 takes the powf branch of the lambda pass's
+# s_corr sum, which the fixtures' n = 4 never reaches.
+STAGE_VARIANTS = ["glsl_stages_scorr.npz:n_corr=3", "glsl_stages_scorr.npz:n_corr=2.5"]
+
+
+def load_stage_fixture(name):
+    if ":" not in name:
+        return H.load(name)
+    base, mod = name.split(":")
+    key, val = mod.split("=")
+    z = H.load(base)
+    z["cfg_" + key] = np.asarray(float(val), dtype=z["cfg_" + key].dtype)
+    return z
+
+
 # ---- substep stages against the oracle (GPU inputs -> FP64) ---------------------------
-@pytest.mark.parametrize("name,mode", [(f, 4) for f in STAGE_FIXTURES] + [(f, 8) for f in STAGE_FIXTURES])
+@pytest.mark.parametrize("name,mode", [(f, m) for m in (4, 8) for f in STAGE_FIXTURES + STAGE_VARIANTS])
 def test_stages_match_oracle(have_gpu, name, mode):
-    z = H.load(name)
+    z = load_stage_fixture(name)
     fl, sdf = make_fluid(z, mode)
     p = H.oracle_params(z)
     S = H.oracle_sdf(z)
